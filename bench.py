@@ -1,0 +1,346 @@
+"""Benchmark of the plain checkerboard sweep: site updates/s and HBM roofline.
+
+Workload (one "step" = one full checkerboard sweep = 4 half-sweeps):
+  480^3 periodic lattice, eps=1, K=1, h=0, kT=0.3, directors uniform on the
+  sphere and chiralities +-1 (Philox seed 11 + rank), d0 = 0.1 with the
+  reference's adaptation, FP64 observables every 100 sweeps.  The float4
+  lattice is 1.77 GB, far above the 126 MB L2, so no L2 flush is needed.
+
+Arms:
+  default            the CUDA library (one process per GPU, independent
+                     replicas, no collective on the data path: weak scaling)
+  --impl reference   the reference algorithm on the host cores (the C oracle
+                     port, OpenMP), each step one sweep of a bounded slab of
+                     the same lattice; rank 0 only.
+
+Prints ONE JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+L_EDGE = 480
+KT, KK, FIELD, EPS, D0, SEED = 0.3, 1.0, 0.0, 1.0, 0.1, 11
+NOUT = 100
+BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
+METRIC = "site_updates_per_s"
+UNIT = "site-updates/s"
+WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
+            f"eps=1 K=1 h=0 kT=0.3, FP64 observables every {NOUT} sweeps")
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"chll_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001 - no nvidia-smi
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+        if getattr(self, "fh", None):
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle port of the reference algorithm on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(seconds: float, threads: int | None = None, nz: int = 8):
+    """Times reference sweeps of a 480 x 480 x nz periodic slab of the workload
+    on the host cores until `seconds` have elapsed (at least one sweep)."""
+    from oracle import oracle as O
+
+    if threads:
+        O.set_threads(threads)
+    cores = O.max_threads()
+    cfg = O.make_cfg(L_EDGE, L_EDGE, nz, periodic=True, kT=KT, K=KK, g=FIELD, eps=EPS,
+                     seed=SEED)
+    nx, ny, nz_, s = O.init_random(cfg)
+    n = L_EDGE * L_EDGE * nz
+    sweeps, t0, step = 0, time.perf_counter(), 1
+    while True:
+        for p in range(4):
+            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+        step += 1
+        sweeps += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
+    return {"value": n * sweeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{sweeps} sweep(s) of a {L_EDGE}x{L_EDGE}x{nz} periodic slab "
+                      f"({n} sites) of the workload, {dt:.1f} s, FP64 reference arithmetic"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    cores = O.max_threads()
+    nz = 8
+    cfg = O.make_cfg(L_EDGE, L_EDGE, nz, periodic=True, kT=KT, K=KK, g=FIELD, eps=EPS, seed=SEED)
+    nx, ny, nz_, s = O.init_random(cfg)
+    n = L_EDGE * L_EDGE * nz
+    step = 1
+    for _ in range(args.warmup):
+        for p in range(4):
+            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+        step += 1
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for p in range(4):
+            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+        times.append(time.perf_counter() - t0)
+        step += 1
+    tot = sum(times)
+    value = n * args.steps / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": [L_EDGE, L_EDGE, L_EDGE],
+                   "sample": f"each step one sweep of a {L_EDGE}x{L_EDGE}x{nz} periodic slab"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} sweeps of a {L_EDGE}x{L_EDGE}x{nz} periodic "
+                                   f"slab ({n} sites); the reference's Fortran/OpenACC build "
+                                   f"needs nvfortran, absent here, so its C restatement runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_arm(args):
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    from chllmodel_b200 import chll
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    n = L_EDGE ** 3
+    cp = coupling(KT, KK, FIELD, EPS)
+    stream = torch.cuda.Stream()
+    lat = Lattice(L_EDGE, L_EDGE, L_EDGE, boundary="periodic")
+    lat.set_stream(stream.cuda_stream)
+    lat.init_random(SEED + rank)
+    lat.set_control(D0, step=1)
+    nmeas = args.steps // NOUT + 2
+    lat.reserve_rows(nmeas)
+
+    # warm-up (captures the 1-sweep graph)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            lat.sweep(cp, 1, seed=SEED, replica=rank)
+        lat.measure(cp, 0)
+    lat.sync()
+    step0 = args.warmup + 1
+
+    ev_start = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    sw_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sw_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clocks:
+        ev_start.record(stream)
+        slot = 0
+        for i in range(args.steps):
+            sw_s[i].record(stream)
+            lat.sweep(cp, 1, seed=SEED, replica=rank)
+            sw_e[i].record(stream)
+            launches += 4
+            if (step0 + i) % NOUT == 0:
+                slot += 1
+                lat.measure(cp, slot)
+                launches += 1
+        ev_end.record(stream)
+        ev_end.synchronize()
+    barrier()
+    ms = ev_start.elapsed_time(ev_end)
+    sweep_ms = sum(a.elapsed_time(b) for a, b in zip(sw_s, sw_e))
+    t = torch.tensor([ms, sweep_ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, sweep_ms = float(t[0]), float(t[1])
+    value = world * n * args.steps / (ms * 1e-3)
+    pass_ms = sweep_ms / (4 * args.steps)
+    achieved_gbs = BYTES_PER_SITE_PASS * n / (pass_ms * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    ctl = lat.control()
+    rows = lat.read_rows(1, slot) if slot else np.zeros((0, 16))
+    lat.close()
+    del lat
+
+    # e2e: the public API with host buffers (pinned), copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        sim = chll.ChLLSim(L_EDGE, L_EDGE, L_EDGE, KT, D0, KK, FIELD, 0.0, seed=SEED + rank,
+                           boundary="periodic", verbose=False)
+        pin = lambda dt: torch.empty((L_EDGE,) * 3, dtype=dt, pin_memory=True).numpy().T
+        sim.nx, sim.ny, sim.nz = pin(torch.float64), pin(torch.float64), pin(torch.float64)
+        sim.s, sim.dope = pin(torch.int32), pin(torch.int32)
+        st = Lattice(L_EDGE, L_EDGE, L_EDGE, boundary="periodic")
+        st.init_random(SEED + rank)
+        x, y, z, sp = st.download_f64()
+        st.close()
+        sim.nx[...], sim.ny[...], sim.nz[...], sim.s[...] = x, y, z, sp
+        del x, y, z, sp
+        nsw = max(args.steps, NOUT)
+        sim.run(NOUT, NOUT)  # warm-up: allocations and graph capture
+        barrier()
+        t0 = time.perf_counter()
+        sim.run(nsw, NOUT)
+        dt = time.perf_counter() - t0
+        tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dt = float(tt[0])
+        h2d = n * (3 * 8 + 4)
+        d2h = n * (3 * 8 + 4) + sim.rows.nbytes
+        e2e = {"value": world * n * nsw / dt, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / nsw, "d2h_bytes_per_step": d2h / nsw,
+               "sweeps": nsw, "api": "ChLLSim.run -> chll_run_ex (C ABI), pinned FP64 host "
+                                     "arrays, upload + pack + sweeps + measurements + unpack + "
+                                     "download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(args.cpu_seconds)
+
+    clk = clocks.summary()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: directors uniform on the sphere, chiralities +-1 p=1/2 "
+                "(Philox seed 11 + rank); state FP32, observables FP64",
+        "config": {"workload": WORKLOAD, "lattice": [L_EDGE, L_EDGE, L_EDGE],
+                   "boundary": "periodic", "kT": KT, "K": KK, "h": FIELD, "eps": EPS,
+                   "d0": D0, "nout": NOUT, "parallelism": f"replicas x{world}",
+                   "l2": "lattice 1.77 GB > 126 MB L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": achieved_gbs / peak, "traffic": None,
+                     "kernel": "sweep_pass_kernel (4 launches per step)",
+                     "bytes_per_launch": BYTES_PER_SITE_PASS * n,
+                     "ms_per_launch": pass_ms, "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "final_control": ctl,
+        "last_row": {"energy_per_site": float(rows[-1][5] / n) if len(rows) else None,
+                     "eta": float(rows[-1][1]) if len(rows) else None},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,186 @@
+// Adjoint of the lattice energy: dE/dn_i for every director and dE/d(eps,K,h).
+//
+// Total energy (each bond once, the sweep's boundary):
+//   E = sum_<ij>, j=i+e_a [ eps*(1 - c^2) - K*c*X*sbar ] - h*sum_i s_i,
+//   c = n_i.n_j,  X = (n_i x n_j).e_a = n_i.(n_j x e_a),  sbar = (s_i+s_j)/2.
+// This is the bond sum behind the reference's local energy (chll_mod.f90:
+// 363-412): the local energy of a site is the sum of the bonds touching it.
+// Per bond, seen from site i with neighbour b in direction sigma*e_a
+// (sigma = -1 forward, +1 backward):
+//   dE_b/dn_i = -2*eps*c*b + sigma*K*sbar*(X*b + c*(b x e_a)),
+// with c = n_i.b and X = (n_i x b).e_a.  The director gradient is optionally
+// projected on the tangent plane, g - (g.n) n/|n|^2 (the torque direction).
+// Coupling derivatives (FP64): dE/deps = sum(1-c^2), dE/dK = -sum(c*X*sbar),
+// dE/dh = -sum(s), together with E itself.
+#include "chll_common.cuh"
+#include "sweep.cuh"
+
+namespace chll {
+
+namespace {
+
+constexpr int kGradThreads = 256;
+constexpr int kGradMaxBlocks = 148 * 4;
+
+__device__ __forceinline__ float4 site(const LatticeView& L, int i, int j, int k) {
+  return L.col[(i + j + k) & 1][((size_t)k * L.nj + j) * L.hx + (i >> 1)];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Adds one bond's dE/dn_i to (gx,gy,gz).  AXIS: 0,1,2; sigma = -1 forward.
+template <int AXIS>
+__device__ __forceinline__ void bond_grad(const float4& n, const float4& b, float sigma,
+                                          const Coupling& cp, float& gx, float& gy, float& gz) {
+  const float c = n.x * b.x + n.y * b.y + n.z * b.z;
+  float X, ex, ey, ez;  // X = (n x b).e_a; (ex,ey,ez) = b x e_a
+  if (AXIS == 0) {
+    X = n.y * b.z - n.z * b.y;
+    ex = 0.f; ey = b.z; ez = -b.y;
+  } else if (AXIS == 1) {
+    X = n.z * b.x - n.x * b.z;
+    ex = -b.z; ey = 0.f; ez = b.x;
+  } else {
+    X = n.x * b.y - n.y * b.x;
+    ex = b.y; ey = -b.x; ez = 0.f;
+  }
+  const float sbar = 0.5f * (n.w + b.w);
+  const float a = -2.f * cp.eps * c;
+  const float w = sigma * cp.K * sbar;
+  gx += a * b.x + w * (X * b.x + c * ex);
+  gy += a * b.y + w * (X * b.y + c * ey);
+  gz += a * b.z + w * (X * b.z + c * ez);
+}
+
+__global__ void __launch_bounds__(kGradThreads)
+    energy_grad_kernel(LatticeView L, Coupling cp, float4* __restrict__ grad_rb, int project,
+                       double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                       double* __restrict__ out4) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};  // E, dE/deps, dE/dK, dE/dh
+  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
+  const size_t total = 2 * per_colour;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int col = e >= per_colour;
+    const size_t t = e - (col ? per_colour : 0);
+    const size_t r = t / (size_t)L.hx;
+    const int h = (int)(t - r * L.hx);
+    const int k = (int)(r / (size_t)L.nj);
+    const int j = (int)(r - (size_t)k * L.nj);
+    const int i = 2 * h + ((col + j + k) & 1);
+    if (i >= L.ni) {
+      if (grad_rb) grad_rb[e] = zero;
+      continue;
+    }
+    const float4 n = L.col[col][t];
+    int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
+    bool hip = ip < L.ni, him = im >= 0, hjp = jp < L.nj, hjm = jm >= 0, hkp = kp < L.nk,
+         hkm = km >= 0;
+    if (L.periodic) {
+      if (!hip) ip = 0;
+      if (!him) im = L.ni - 1;
+      if (!hjp) jp = 0;
+      if (!hjm) jm = L.nj - 1;
+      if (!hkp) kp = 0;
+      if (!hkm) km = L.nk - 1;
+      hip = him = hjp = hjm = hkp = hkm = true;
+    }
+    const float4 bxp = hip ? site(L, ip, j, k) : zero;
+    const float4 bxm = him ? site(L, im, j, k) : zero;
+    const float4 byp = hjp ? site(L, i, jp, k) : zero;
+    const float4 bym = hjm ? site(L, i, jm, k) : zero;
+    const float4 bzp = hkp ? site(L, i, j, kp) : zero;
+    const float4 bzm = hkm ? site(L, i, j, km) : zero;
+
+    if (grad_rb) {
+      float gx = 0.f, gy = 0.f, gz = 0.f;
+      bond_grad<0>(n, bxp, -1.f, cp, gx, gy, gz);
+      bond_grad<0>(n, bxm, +1.f, cp, gx, gy, gz);
+      bond_grad<1>(n, byp, -1.f, cp, gx, gy, gz);
+      bond_grad<1>(n, bym, +1.f, cp, gx, gy, gz);
+      bond_grad<2>(n, bzp, -1.f, cp, gx, gy, gz);
+      bond_grad<2>(n, bzm, +1.f, cp, gx, gy, gz);
+      if (project) {
+        const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+        const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
+        gx -= gn * n.x;
+        gy -= gn * n.y;
+        gz -= gn * n.z;
+      }
+      grad_rb[e] = make_float4(gx, gy, gz, 0.f);
+    }
+
+    // FP64 forward-bond sums (each bond once).
+    const double nx = n.x, ny = n.y, nz = n.z, s = n.w;
+    const float4* fw[3] = {&bxp, &byp, &bzp};
+    const bool hf[3] = {hip, hjp, hkp};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (!hf[a]) continue;
+      const float4 b = *fw[a];
+      const double c = nx * b.x + ny * b.y + nz * b.z;
+      const double X = (a == 0) ? ny * b.z - nz * b.y
+                     : (a == 1) ? nz * b.x - nx * b.z
+                                : nx * b.y - ny * b.x;
+      const double sbar = 0.5 * (s + (double)b.w);
+      const double nem = 1.0 - c * c;
+      const double chi = -c * X * sbar;
+      acc[0] += (double)cp.eps * nem + (double)cp.K * chi;
+      acc[1] += nem;
+      acc[2] += chi;
+    }
+    acc[0] -= (double)cp.g * s;
+    acc[3] -= s;
+  }
+
+  __shared__ double s_part[kGradThreads / 32][4];
+  __shared__ bool s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const double v = warp_sum(acc[m]);
+    if (lane == 0) s_part[warp][m] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int w = 0; w < kGradThreads / 32; ++w) v += s_part[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * 4 + threadIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (unsigned int b = 0; b < gridDim.x; ++b)
+      v += *((volatile double*)&partials[(size_t)b * 4 + threadIdx.x]);
+    out4[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *ticket = 0;
+}
+
+}  // namespace
+
+int energy_grad_max_blocks() { return kGradMaxBlocks; }
+
+void launch_energy_grad(const LatticeView& L, const Coupling& cp, float4* grad_rb, int project,
+                        double* partials, unsigned int* ticket, double* out4,
+                        cudaStream_t stream) {
+  const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;
+  size_t blocks = (total + kGradThreads - 1) / kGradThreads;
+  if (blocks > (size_t)kGradMaxBlocks) blocks = kGradMaxBlocks;
+  if (blocks == 0) blocks = 1;
+  energy_grad_kernel<<<(unsigned int)blocks, kGradThreads, 0, stream>>>(
+      L, cp, grad_rb, project, partials, ticket, out4);
+}
+
+}  // namespace chll

@@ -1,0 +1,130 @@
+// Shared device/host definitions of the B200 chiral Lebwohl-Lasher library:
+// the counter-based random stream, the red/black float4 lattice view, the
+// coupling constants and the per-replica control block that the sweep
+// kernels update on the device.
+//
+// Physics (restated from the reference module chll/chll_mod.f90):
+//   local energy of site i with director n and chirality s
+//     E_i = sum_b [ eps*(1 - (n.n_b)^2) + sigma_b*K*(n.n_b)*((n x n_b).e_b)*(s+s_b)/2 ] - g*s
+//   over the six neighbours b, sigma_b = -1 for the +axis neighbour and +1
+//   for the -axis neighbour (chll_mod.f90:363-412; eps = 1 in the reference).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace chll {
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel Random Numbers: As Easy
+// as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies with the
+// published multipliers, the key bumped by the published Weyl increments
+// between rounds.  Counters used by this library:
+//   sweep passes : {group, step, replica, pass}   pass = 0..3 (see Pass)
+//   random init  : {site,  0xffffffff, replica, kStreamInit}
+// where group = (i>>2) + (ceil(ni/4)) * (j + nj*k) is the index of the
+// 4-site x-block holding the site (two sites of each colour), and
+// site = i + ni*(j + nj*k) (0-based, F-order).
+// ---------------------------------------------------------------------------
+struct Ctr4 {
+  uint32_t v[4];
+};
+
+__host__ __device__ __forceinline__ Ctr4 philox4x32_10(Ctr4 c, uint32_t k0, uint32_t k1) {
+  constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;
+  constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)kM0 * c.v[0];
+    const uint64_t p1 = (uint64_t)kM1 * c.v[2];
+    Ctr4 n;
+    n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ k0;
+    n.v[1] = (uint32_t)p1;
+    n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1;
+    n.v[3] = (uint32_t)p0;
+    c = n;
+    k0 += kW0;
+    k1 += kW1;
+  }
+  return c;
+}
+
+// Top 24 bits of a word as a uniform in [0,1): exact in FP32 and FP64, so the
+// host oracle and the device read identical numbers.
+__host__ __device__ __forceinline__ float u01(uint32_t x) {
+  return (float)(x >> 8) * 5.9604644775390625e-8f;  // 2^-24
+}
+
+enum Pass : uint32_t {
+  kPassDir0 = 0,   // director trials on colour 0 (reference sublattice sl1)
+  kPassDir1 = 1,   // director trials on colour 1 (sl2)
+  kPassSpin0 = 2,  // chirality flips on colour 0
+  kPassSpin1 = 3,  // chirality flips on colour 1
+  kStreamInit = 4  // random initial state
+};
+
+// ---------------------------------------------------------------------------
+// Red/black float4 lattice.  Site (i,j,k), 0-based, has colour
+// c = (i+j+k)&1; colour 0 is the reference's "odd" sublattice sl1 (1-based
+// i+j+k odd, chll_mod.f90:27).  Each colour is a dense array
+//   col[c][(k*nj + j)*hx + h],   i = 2h + ((c+j+k)&1),
+// of float4 (nx, ny, nz, s) with hx = ni_p/2 and ni_p = ni rounded up to a
+// multiple of 4.  Storage slots with i >= ni are padding, held at zero.
+// ---------------------------------------------------------------------------
+struct LatticeView {
+  float4* col[2];
+  int ni, nj, nk;
+  int hx;        // storage half-row length (even)
+  int periodic;  // 0: open boundaries (reference sweep), 1: periodic
+};
+
+__host__ __device__ __forceinline__ int padded_ni(int ni) { return (ni + 3) & ~3; }
+
+struct Coupling {
+  float eps;     // nematic coupling (reference: 1)
+  float K;       // chiral coupling KK
+  float g;       // field on the chirality
+  float inv_kT;  // 1/kT (+inf at kT = 0, as the reference's division gives)
+};
+
+// Per-replica control block, resident in device memory so that graph-captured
+// sweep loops need no host round trip (chll_mod.f90:62-90).
+struct Control {
+  double d;                  // proposal amplitude (reference: d, FP64)
+  long long step;            // step number of the sweep in progress
+  long long adapt_until;     // d is adapted after sweeps with step < adapt_until
+  long long nsites;          // real site count ni*nj*nk
+  unsigned long long nacc;   // director accepts in the current sweep
+  unsigned long long nflip;  // chirality flips in the current sweep
+  unsigned int done;         // blocks finished in the current pass
+  unsigned int status;       // nonzero: device-detected error
+  float paccept;             // accepted director fraction of the last sweep
+  float faccept;             // accepted flip fraction of the last sweep
+  long long nacc_last;       // raw counts of the last sweep
+  long long nflip_last;
+};
+
+// Row written by the observables kernel (FP64).  Columns 0-4 are the
+// reference's measurement row m(r,1:5) (chll_mod.f90:99-104).
+enum RowCol : int {
+  kRowEtotRef = 0,  // etot() per site, reference boundary quirks, FP32-rounded
+  kRowEta = 1,      // sum(s)/N in FP32
+  kRowPaccept = 2,
+  kRowFaccept = 3,
+  kRowD = 4,
+  kRowEnergy = 5,   // total energy (sweep boundary), FP64
+  kRowSumS = 6,     // sum of s
+  kRowQxx = 7,      // sum nx*nx ... (Q-tensor raw moments)
+  kRowQyy = 8,
+  kRowQzz = 9,
+  kRowQxy = 10,
+  kRowQxz = 11,
+  kRowQyz = 12,
+  kRowEtotRefSum = 13,  // FP64 sum behind column 0
+  kRowStep = 14,
+  kRowNsites = 15,
+  kRowLen = 16
+};
+
+constexpr int kObsMoments = 9;  // E, E_ref, sum s, 6 Q sums
+
+}  // namespace chll

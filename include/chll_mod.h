@@ -1,0 +1,175 @@
+/*
+ * chll_mod.h -- C ABI of libchll_mod.so, the B200 (sm_100a) chiral
+ * Lebwohl-Lasher checkerboard Metropolis library.
+ *
+ * The first two entry points are the reference's own ctypes boundary and are
+ * drop-in replacements for the nvfortran-built libchll_mod.so:
+ *   init  <- chll/chll_mod.f90:9-14   (bind(c, name="init")),
+ *            bound by ftn_init in chll/chll.py:9-18
+ *   run   <- chll/chll_mod.f90:40-48  (bind(c, name="run")),
+ *            bound by ftn_run in chll/chll.py:20-36
+ * Every scalar is passed by reference, arrays are Fortran-ordered (i fastest)
+ * and owned by the caller, exactly as the Fortran interface expects.
+ *
+ * The chll_* entry points are extensions with the same conventions (plain
+ * pointers and sizes, caller-owned buffers).  They return 0 on success and a
+ * nonzero CHLL_E* code on failure; chll_last_error() then describes it.  The
+ * reference's void entry points report failures the same way (status +
+ * message on stderr) instead of aborting the host process.
+ *
+ * The library runs on the current CUDA device, one stream per lattice, and is
+ * not re-entrant across threads for the same lattice; init/run serialise on an
+ * internal mutex.
+ */
+#ifndef CHLL_MOD_H
+#define CHLL_MOD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CHLL_OK 0
+#define CHLL_EINVAL 1    /* invalid argument (null pointer, bad size, odd periodic dim) */
+#define CHLL_ECUDA 2     /* CUDA runtime error */
+#define CHLL_ENOMEM 3    /* device allocation failed */
+#define CHLL_EDEVICE 4   /* device-side status word was set */
+#define CHLL_ERANGE 5    /* more measurement rows than the caller's buffers hold */
+
+#define CHLL_OPEN 0      /* open boundaries: the reference sweep (chll_mod.f90:371-410) */
+#define CHLL_PERIODIC 1  /* periodic boundaries (requires even ni, nj, nk) */
+
+/* Columns of a measurement row (FP64).  0-4 are the reference's m(r,1:5)
+ * (chll_mod.f90:99-104): etot, e_excess, paccept, faccept, d. */
+#define CHLL_ROW_ETOT 0
+#define CHLL_ROW_ETA 1
+#define CHLL_ROW_PACCEPT 2
+#define CHLL_ROW_FACCEPT 3
+#define CHLL_ROW_D 4
+#define CHLL_ROW_ENERGY 5        /* total energy, sweep boundary, FP64 */
+#define CHLL_ROW_SUM_S 6         /* sum of chiralities */
+#define CHLL_ROW_QXX 7           /* raw sums of n_a n_b: xx yy zz xy xz yz (7..12) */
+#define CHLL_ROW_ETOT_SUM 13     /* FP64 sum behind column 0 */
+#define CHLL_ROW_STEP 14
+#define CHLL_ROW_NSITES 15
+#define CHLL_ROW_LEN 16
+
+/* ---- reference entry points -------------------------------------------- */
+
+/* Builds the checkerboard index lists: sl1 gets the 1-based F-order indices of
+ * sites with (i+j+k) odd (1-based i,j,k), sl2 the rest, each of length nsub.
+ * nx..dope are accepted and left untouched, as in the reference.
+ * Replaces chll_mod.f90:9-38. */
+void init(double* nx, double* ny, double* nz, int* s, int* dope, int* sl1, int* sl2,
+          const int* ni, const int* nj, const int* nk, const int* nsub);
+
+/* Runs steps nstart..nstop (one step = director half-sweeps on sl1 then sl2,
+ * chirality half-sweeps on sl1 then sl2) on the GPU with open boundaries,
+ * adapting d while step < 10000, and measures every nout steps into
+ * msteps[r] and m (F-order rows x 5, rows = (1+nstop-nstart)/nout).  Prints
+ * the reference's stdout table.  The final state is written back into
+ * nx, ny, nz, s; d receives the adapted step size and nsub = N/2.
+ * Random numbers: Philox4x32-10 keyed by the seed of chll_set_seed (default 1)
+ * and the ordinal of this run() call since that seed was set.
+ * sl1, sl2, dope are accepted and not used (the lattice is red/black on the
+ * device).  Replaces chll_mod.f90:40-115. */
+void run(const int* nstart, const int* nstop, const int* nout, double* nx, double* ny,
+         double* nz, int* s, int* dope, int* sl1, int* sl2, double* g, double* KK, double* d,
+         double* kbt, const int* ni, const int* nj, const int* nk, int* nsub, int* msteps,
+         double* m);
+
+/* ---- errors and seeding ------------------------------------------------- */
+
+/* Status of the last call made on this thread (CHLL_OK if it succeeded). */
+int chll_last_status(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* chll_last_error(void);
+/* Seed of the Philox stream used by run(); resets the run() ordinal. */
+void chll_set_seed(uint64_t seed);
+/* Library version string. */
+const char* chll_version(void);
+
+/* ---- extended run (same semantics as run, explicit options) ------------- */
+
+typedef struct chll_run_config {
+  double kT;            /* temperature kbt */
+  double K;             /* chiral coupling KK */
+  double g;             /* field on the chirality */
+  double eps;           /* nematic coupling; 1 reproduces the reference */
+  double d;             /* initial proposal amplitude */
+  uint64_t seed;        /* Philox key */
+  uint32_t replica;     /* Philox counter word 2 */
+  int32_t boundary;     /* CHLL_OPEN or CHLL_PERIODIC */
+  int64_t adapt_until;  /* d adapted after steps < adapt_until (reference: 10000) */
+  int32_t verbose;      /* nonzero: print the reference's stdout table */
+  int32_t reserved;
+} chll_run_config;
+
+/* run() with explicit options.  m (rows x 5, F-order) and rows16 (rows x
+ * CHLL_ROW_LEN, C-order) are optional.  d_out receives the final d.
+ * Fails with CHLL_ERANGE (after running) if more steps in nstart..nstop are
+ * multiples of nout than the (1+nstop-nstart)/nout rows the buffers hold. */
+int chll_run_ex(const chll_run_config* cfg, int nstart, int nstop, int nout, double* nx,
+                double* ny, double* nz, int* s, int ni, int nj, int nk, int* msteps, double* m,
+                double* rows16, double* d_out);
+
+/* ---- device-resident lattices (bench, autograd, workflows) -------------- */
+
+typedef struct chll_lattice chll_lattice;
+
+typedef struct chll_coupling {
+  double kT, K, g, eps;
+} chll_coupling;
+
+/* Allocates a red/black float4 lattice of ni x nj x nk sites on the current
+ * device (about 16 bytes per site). */
+int chll_lattice_create(int ni, int nj, int nk, int boundary, chll_lattice** out);
+void chll_lattice_destroy(chll_lattice* lat);
+/* Launch stream for all work on this lattice (a cudaStream_t; NULL restores
+ * the lattice's own stream). */
+int chll_lattice_set_stream(chll_lattice* lat, void* stream);
+int chll_lattice_sync(chll_lattice* lat);
+/* Random initial state: directors uniform on the sphere, s = +-1 with p=1/2. */
+int chll_lattice_init_random(chll_lattice* lat, uint64_t seed, uint32_t replica);
+/* F-order FP64 directors and int32 spins, host or device pointers. */
+int chll_lattice_upload_f64(chll_lattice* lat, const double* nx, const double* ny,
+                            const double* nz, const int* s);
+int chll_lattice_download_f64(chll_lattice* lat, double* nx, double* ny, double* nz, int* s);
+/* Natural-order (i fastest) float4 (nx, ny, nz, s) records, host or device. */
+int chll_lattice_upload_f4(chll_lattice* lat, const float* xyzs);
+int chll_lattice_download_f4(chll_lattice* lat, float* xyzs);
+/* Red/black storage: colour c array base (device) and its length in float4. */
+int chll_lattice_storage(chll_lattice* lat, void** colour0, void** colour1, int64_t* per_colour,
+                         int32_t* hx);
+/* Device control block: d, step, adaptation limit. */
+int chll_lattice_set_control(chll_lattice* lat, double d, int64_t step, int64_t adapt_until);
+int chll_lattice_get_control(chll_lattice* lat, double* d, int64_t* step, double* paccept,
+                             double* faccept);
+/* nsweeps full steps (4 half-sweeps each) from the control block's step.
+ * Consecutive calls with the same count replay one captured CUDA graph. */
+int chll_lattice_sweep(chll_lattice* lat, const chll_coupling* c, uint64_t seed,
+                       uint32_t replica, int nsweeps);
+/* One half-sweep: pass 0/1 director colour 0/1, 2/3 chirality colour 0/1. */
+int chll_lattice_pass(chll_lattice* lat, const chll_coupling* c, uint64_t seed,
+                      uint32_t replica, int pass);
+/* Device measurement rows: reserve room for n rows, enqueue the FP64
+ * observables of the current state into row `slot` without waiting, and read
+ * rows [first, first+count) back to the host (waits for the stream). */
+int chll_lattice_reserve_rows(chll_lattice* lat, int n);
+int chll_lattice_measure(chll_lattice* lat, const chll_coupling* c, int slot);
+int chll_lattice_read_rows(chll_lattice* lat, double* rows16, int first, int count);
+/* FP64 observables into a host row of CHLL_ROW_LEN doubles. */
+int chll_lattice_observe(chll_lattice* lat, const chll_coupling* c, double* row16);
+/* Energy adjoint: grad (natural order float4, host or device, may be NULL)
+ * receives dE/dn_i (w = 0), tangent-projected if project != 0; out4 (host)
+ * receives {E, dE/deps, dE/dK, dE/dh} in FP64. */
+int chll_lattice_energy_grad(chll_lattice* lat, const chll_coupling* c, float* grad, int project,
+                             double* out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHLL_MOD_H */
