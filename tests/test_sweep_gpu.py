@@ -44,10 +44,10 @@ def lockstep(oracle, shape, periodic, kT, K, g, eps=1.0, sweeps=3, seed=5, d0=0.
         for p in range(4):
             ctl = lat.control()
             state = lat.download_f64()
-            before = [a.copy() for a in state]
+            before = [a.copy(order="F") for a in state]
             lat.half_sweep(cp, p, seed=seed)
             after = lat.download_f64()
-            onx, ony, onz, os_ = [a.copy() for a in before]
+            onx, ony, onz, os_ = [a.copy(order="F") for a in before]
             d32 = float(np.float32(ctl["d"]))
             n, acc, de, u = oracle.run_pass(cfg, p, ctl["step"], d32, onx, ony, onz, os_,
                                             detail=True)
