@@ -30,7 +30,7 @@ EXPORTS = (
     "chll_lattice_storage", "chll_lattice_set_control", "chll_lattice_get_control",
     "chll_lattice_sweep", "chll_lattice_pass", "chll_lattice_observe",
     "chll_lattice_energy_grad", "chll_lattice_reserve_rows", "chll_lattice_measure",
-    "chll_lattice_read_rows",
+    "chll_lattice_read_rows", "chll_energy_grad_noalloc",
 )
 
 
@@ -144,6 +144,9 @@ def _declare(L: ct.CDLL) -> None:
                  "chll_lattice_observe", "chll_lattice_energy_grad", "chll_lattice_reserve_rows",
                  "chll_lattice_measure", "chll_lattice_read_rows"):
         getattr(L, name).restype = i32
+    L.chll_energy_grad_noalloc.argtypes = [vp, vp, i32, i32, i32, i32, P(Coupling), i32, vp, vp,
+                                           vp]
+    L.chll_energy_grad_noalloc.restype = i32
     if hasattr(L, "chll_batch_create"):
         L.chll_batch_create.argtypes = [P(ReplicaSpec), i32, P(vp)]
         L.chll_batch_create.restype = i32

@@ -109,6 +109,12 @@ int check_device() {
 
 }  // namespace
 
+namespace chll {
+// Error recording for entry points defined in other translation units.
+int record_error(int code, const char* msg) { return fail(code, "%s", msg); }
+int record_ok() { return ok(); }
+}  // namespace chll
+
 // ---------------------------------------------------------------------------
 // Lattice object
 // ---------------------------------------------------------------------------

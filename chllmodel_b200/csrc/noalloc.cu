@@ -1,0 +1,167 @@
+// Energy adjoint with no device allocation: chll_energy_grad_noalloc.
+//
+// chll_lattice_energy_grad allocates (cudaMalloc) a red/black gradient buffer
+// as large as the lattice the first time it runs, and keeps its reduction
+// partials in the lattice object.  Some callers cannot let a library allocate
+// device memory: a Fortran/OpenACC host (the reference's own kind of program)
+// whose arrays live in its runtime's device pool, or an application that has
+// handed nearly all of HBM to its own allocator, where a cudaMalloc either
+// fails or competes with the owner's pool.  This entry point takes the
+// caller's device buffers for the lattice and the results, and runs the same
+// adjoint and unpack kernels with every intermediate buffer placed in one
+// fixed array of this file:
+//
+//   g_noalloc_scratch = [ red/black gradient, at most kMaxSlots float4 ]
+//                       [ per-CTA partial sums, kPartials doubles       ]
+//                       [ completion ticket                              ]
+//
+// kMaxSlots = 262,144 float4 slots (4 MiB), enough for a 64^3 lattice;
+// the whole array is about 4.02 MiB and every GPU that loads the library
+// holds it until the process exits.
+//
+// The host cannot use the array's name as a device address.  The first call
+// on each device asks the runtime for the address (cudaGetSymbolAddress, with
+// that device current), caches it, and passes it to the kernels; make that
+// first call before any stream capture.  All calls share the array and it
+// keeps the last call's contents: the completion ticket is cleared at the
+// start of every call, everything else is fully rewritten before it is read.
+// Two calls whose work overlaps on the GPU (different streams, or different
+// host threads on the same device) race on the array and give wrong results;
+// serialise them.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/chll_mod.h"
+#include "chll_common.cuh"
+#include "sweep.cuh"
+
+namespace chll {
+int record_error(int code, const char* msg);
+int record_ok();
+}  // namespace chll
+
+namespace {
+
+constexpr size_t kMaxSlots = 2ull * 32 * 64 * 64;  // red/black slots of a 64^3 lattice
+constexpr size_t kPartials = 148ull * 4 * 4;        // energy_grad_max_blocks() x 4 sums
+constexpr size_t kGradBytes = kMaxSlots * sizeof(float4);
+constexpr size_t kPartialBytes = kPartials * sizeof(double);
+constexpr size_t kScratchBytes = kGradBytes + kPartialBytes + 256;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+std::mutex g_setup_mutex;
+unsigned char* g_scratch_addr[kMaxDevices] = {};
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return chll::record_error(code, buf);
+}
+
+bool on_device(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Device address of g_noalloc_scratch on the current device (set up once).
+int scratch_address(unsigned char** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CHLL_ECUDA, "energy_grad_noalloc: no CUDA device available (%s)",
+                cudaGetErrorString(e));
+  }
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: device ordinal %d >= %d", dev, kMaxDevices);
+  std::lock_guard<std::mutex> lk(g_setup_mutex);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return fail(CHLL_ECUDA, "energy_grad_noalloc: cudaGetSymbolAddress failed on device %d: %s",
+                  dev, cudaGetErrorString(e));
+    }
+    g_scratch_addr[dev] = (unsigned char*)p;
+  }
+  *out = g_scratch_addr[dev];
+  return CHLL_OK;
+}
+
+}  // namespace
+
+extern "C" int chll_energy_grad_noalloc(const void* colour0, const void* colour1, int ni, int nj,
+                                        int nk, int boundary, const chll_coupling* c,
+                                        int project, float* grad, double* out4, void* stream) {
+  if (!colour0 || !colour1 || !c || !out4)
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: null lattice, coupling or out4");
+  if (ni < 1 || nj < 1 || nk < 1)
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: dims must be >= 1 (got %d %d %d)", ni, nj, nk);
+  if (boundary != CHLL_OPEN && boundary != CHLL_PERIODIC)
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: boundary must be CHLL_OPEN or CHLL_PERIODIC");
+  if (boundary == CHLL_PERIODIC && ((ni | nj | nk) & 1))
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: periodic boundaries need even dims");
+  const int hx = chll::padded_ni(ni) / 2;
+  const size_t per_colour = (size_t)hx * nj * nk;
+  if (2 * per_colour > kMaxSlots)
+    return fail(CHLL_ERANGE,
+                "energy_grad_noalloc: a %dx%dx%d lattice needs %zu red/black slots; the fixed "
+                "scratch holds at most %zu (a 64^3 lattice). Use chll_lattice_energy_grad, "
+                "which allocates.",
+                ni, nj, nk, 2 * per_colour, kMaxSlots);
+  if (chll::energy_grad_max_blocks() * 4 > (int)kPartials)
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: partial-sum scratch too small");
+  if (!on_device(colour0) || !on_device(colour1) || !on_device(out4) ||
+      (grad && !on_device(grad)))
+    return fail(CHLL_EINVAL, "energy_grad_noalloc: lattice, grad and out4 must be device memory");
+
+  unsigned char* base = nullptr;
+  const int rc = scratch_address(&base);
+  if (rc != CHLL_OK) return rc;
+  float4* grad_rb = (float4*)base;
+  double* partials = (double*)(base + kGradBytes);
+  unsigned int* ticket = (unsigned int*)(base + kGradBytes + kPartialBytes);
+  cudaStream_t s = (cudaStream_t)stream;
+
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess)
+    return fail(CHLL_ECUDA, "energy_grad_noalloc: %s", cudaGetErrorString(e));
+
+  chll::LatticeView v;
+  v.col[0] = (float4*)colour0;
+  v.col[1] = (float4*)colour1;
+  v.ni = ni;
+  v.nj = nj;
+  v.nk = nk;
+  v.hx = hx;
+  v.periodic = boundary;
+  chll::Coupling cp;
+  cp.eps = (float)c->eps;
+  cp.K = (float)c->K;
+  cp.g = (float)c->g;
+  cp.inv_kT = (float)(1.0 / c->kT);
+  chll::launch_energy_grad(v, cp, grad ? grad_rb : nullptr, project, partials, ticket, out4, s);
+  if (grad) {
+    chll::LatticeView gv = v;
+    gv.col[0] = grad_rb;
+    gv.col[1] = grad_rb + per_colour;
+    chll::launch_unpack_f4(gv, (float4*)grad, s);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(CHLL_ECUDA, "energy_grad_noalloc: launch failed: %s", cudaGetErrorString(e));
+  return chll::record_ok();
+}

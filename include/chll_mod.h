@@ -168,6 +168,29 @@ int chll_lattice_observe(chll_lattice* lat, const chll_coupling* c, double* row1
 int chll_lattice_energy_grad(chll_lattice* lat, const chll_coupling* c, float* grad, int project,
                              double* out4);
 
+/* ---- energy adjoint without device allocation --------------------------- */
+
+/* Same results as chll_lattice_energy_grad, for callers that cannot let a
+ * library call cudaMalloc (a Fortran/OpenACC host whose arrays live in its
+ * runtime's device pool, or an application whose own allocator holds nearly
+ * all of HBM).  No counterpart in the reference.
+ *   colour0, colour1: device red/black lattice arrays, each hx*nj*nk float4
+ *     with hx = 2*ceil(ni/4), slot (k*nj + j)*hx + (i>>1) holding site
+ *     (i,j,k) of colour (i+j+k)&1, padding slots zero (the layout
+ *     chll_lattice_storage exposes);
+ *   grad: device, natural order (i fastest) ni*nj*nk float4, may be NULL;
+ *   out4: device, 4 doubles {E, dE/deps, dE/dK, dE/dh};
+ *   stream: cudaStream_t the work is enqueued on (asynchronous).
+ * All intermediates live in one fixed device array of this library (about
+ * 4 MiB on every GPU that loads it, held until exit): lattices needing more
+ * than 262,144 red/black slots (2*hx*nj*nk; a 64^3 lattice fits) are rejected
+ * with CHLL_ERANGE.  The first call on each device looks up that array's
+ * device address; make it before any stream capture.  Calls share the array:
+ * calls whose work overlaps on the GPU race and must be serialised. */
+int chll_energy_grad_noalloc(const void* colour0, const void* colour1, int ni, int nj, int nk,
+                             int boundary, const chll_coupling* c, int project, float* grad,
+                             double* out4, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

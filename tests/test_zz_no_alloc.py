@@ -1,0 +1,71 @@
+"""The no-allocation energy adjoint, chll_energy_grad_noalloc, called through
+the C ABI, against the allocating chll_lattice_energy_grad.
+
+It exists for callers that cannot let a library call cudaMalloc -- a
+Fortran/OpenACC host whose arrays live in its runtime's device pool, or an
+application whose own allocator holds nearly all of HBM -- so it keeps every
+intermediate in one fixed device array of the library.  This file is
+collected last: two calls in a row must each reproduce the allocating entry
+point, and a lattice larger than the fixed array must be refused."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 2e-5   # the adjoint tests' tolerance for the FP32 gradient
+GRAD_ATOL = 2e-5
+SUM_RTOL = 1e-9    # and for the FP64 sums
+
+
+@pytest.mark.parametrize("shape,boundary", [((64, 64, 64), "periodic"),
+                                            ((37, 20, 12), "open")])
+def test_noalloc_adjoint_matches_allocating_entry_point(shape, boundary):
+    import torch
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    L = _lib.load()
+    lat = Lattice(*shape, boundary=boundary)
+    lat.init_random(seed=5)
+    cp = coupling(0.3, 1.0, 0.5, 1.1)
+    lat.set_control(0.1, step=1)
+    lat.sweep(cp, 4, seed=5)
+    ref_grad, ref_out4 = lat.energy_grad(cp, project=True)   # allocating entry point
+    c0, c1, _, _ = lat.storage()
+    n = lat.nsites
+    grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    out4 = torch.empty(4, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    bnd = _lib.CHLL_PERIODIC if boundary == "periodic" else _lib.CHLL_OPEN
+    for _ in range(2):
+        grad.fill_(float("nan"))
+        out4.fill_(float("nan"))
+        rc = L.chll_energy_grad_noalloc(ct.c_void_p(c0), ct.c_void_p(c1), *shape, bnd,
+                                        ct.byref(cp), 1, ct.c_void_p(grad.data_ptr()),
+                                        ct.c_void_p(out4.data_ptr()), ct.c_void_p(stream))
+        _lib.check(rc)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(grad.cpu().numpy(), ref_grad, rtol=GRAD_RTOL, atol=GRAD_ATOL)
+        np.testing.assert_allclose(out4.cpu().numpy(), ref_out4, rtol=SUM_RTOL, atol=SUM_RTOL)
+    lat.close()
+
+
+def test_noalloc_adjoint_refuses_lattices_beyond_its_scratch():
+    import torch
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    L = _lib.load()
+    lat = Lattice(66, 64, 64, boundary="periodic")   # 2*34*64*64 slots > 262,144
+    c0, c1, _, _ = lat.storage()
+    out4 = torch.empty(4, dtype=torch.float64, device="cuda")
+    rc = L.chll_energy_grad_noalloc(ct.c_void_p(c0), ct.c_void_p(c1), 66, 64, 64,
+                                    _lib.CHLL_PERIODIC, ct.byref(coupling(0.3, 1.0)), 0, None,
+                                    ct.c_void_p(out4.data_ptr()), None)
+    assert rc == _lib.CHLL_ERANGE
+    assert "at most 262144" in _lib.last_error()
+    lat.close()
