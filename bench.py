@@ -202,10 +202,11 @@ def gpu_arm(args):
     from chllmodel_b200 import chll
     from chllmodel_b200.lattice import Lattice, coupling
 
-    n = L_EDGE ** 3
+    edge = args.edge
+    n = edge ** 3
     cp = coupling(KT, KK, FIELD, EPS)
     stream = torch.cuda.Stream()
-    lat = Lattice(L_EDGE, L_EDGE, L_EDGE, boundary="periodic")
+    lat = Lattice(edge, edge, edge, boundary="periodic")
     lat.set_stream(stream.cuda_stream)
     lat.init_random(SEED + rank)
     lat.set_control(D0, step=1)
@@ -259,12 +260,12 @@ def gpu_arm(args):
     # e2e: the public API with host buffers (pinned), copies inside the timed region
     e2e = None
     if not args.no_e2e:
-        sim = chll.ChLLSim(L_EDGE, L_EDGE, L_EDGE, KT, D0, KK, FIELD, 0.0, seed=SEED + rank,
+        sim = chll.ChLLSim(edge, edge, edge, KT, D0, KK, FIELD, 0.0, seed=SEED + rank,
                            boundary="periodic", verbose=False)
-        pin = lambda dt: torch.empty((L_EDGE,) * 3, dtype=dt, pin_memory=True).numpy().T
+        pin = lambda dt: torch.empty((edge,) * 3, dtype=dt, pin_memory=True).numpy().T
         sim.nx, sim.ny, sim.nz = pin(torch.float64), pin(torch.float64), pin(torch.float64)
         sim.s, sim.dope = pin(torch.int32), pin(torch.int32)
-        st = Lattice(L_EDGE, L_EDGE, L_EDGE, boundary="periodic")
+        st = Lattice(edge, edge, edge, boundary="periodic")
         st.init_random(SEED + rank)
         x, y, z, sp = st.download_f64()
         st.close()
@@ -304,10 +305,11 @@ def gpu_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: directors uniform on the sphere, chiralities +-1 p=1/2 "
                 "(Philox seed 11 + rank); state FP32, observables FP64",
-        "config": {"workload": WORKLOAD, "lattice": [L_EDGE, L_EDGE, L_EDGE],
+        "config": {"workload": WORKLOAD if edge == L_EDGE else WORKLOAD.replace(
+                       f"{L_EDGE}^3", f"{edge}^3"), "lattice": [edge, edge, edge],
                    "boundary": "periodic", "kT": KT, "K": KK, "h": FIELD, "eps": EPS,
                    "d0": D0, "nout": NOUT, "parallelism": f"replicas x{world}",
-                   "l2": "lattice 1.77 GB > 126 MB L2; no flush"},
+                   "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak, "traffic": None,
                      "kernel": "sweep_pass_kernel (4 launches per step)",
@@ -334,6 +336,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--edge", type=int, default=L_EDGE,
+                    help="lattice edge (480 is the benchmark; smaller edges for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

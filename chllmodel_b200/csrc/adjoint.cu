@@ -57,9 +57,14 @@ __device__ __forceinline__ void bond_grad(const float4& n, const float4& b, floa
 }
 
 __global__ void __launch_bounds__(kGradThreads)
-    energy_grad_kernel(LatticeView L, Coupling cp, float4* __restrict__ grad_rb, int project,
+    energy_grad_kernel(LatticeView L, CouplingD cd, float4* __restrict__ grad_rb, int project,
                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
                        double* __restrict__ out4) {
+  Coupling cp;  // FP32 couplings of the per-site gradient
+  cp.eps = (float)cd.eps;
+  cp.K = (float)cd.K;
+  cp.g = (float)cd.g;
+  cp.inv_kT = 0.f;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};  // E, dE/deps, dE/dK, dE/dh
   const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
   const size_t total = 2 * per_colour;
@@ -130,11 +135,11 @@ __global__ void __launch_bounds__(kGradThreads)
       const double sbar = 0.5 * (s + (double)b.w);
       const double nem = 1.0 - c * c;
       const double chi = -c * X * sbar;
-      acc[0] += (double)cp.eps * nem + (double)cp.K * chi;
+      acc[0] += cd.eps * nem + cd.K * chi;
       acc[1] += nem;
       acc[2] += chi;
     }
-    acc[0] -= (double)cp.g * s;
+    acc[0] -= cd.g * s;
     acc[3] -= s;
   }
 
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(kGradThreads)
 
 int energy_grad_max_blocks() { return kGradMaxBlocks; }
 
-void launch_energy_grad(const LatticeView& L, const Coupling& cp, float4* grad_rb, int project,
+void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,
                         double* partials, unsigned int* ticket, double* out4,
                         cudaStream_t stream) {
   const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;

@@ -83,6 +83,14 @@ Coupling make_coupling(const chll_coupling& c) {
   return cp;
 }
 
+chll::CouplingD make_coupling_d(const chll_coupling& c) {
+  chll::CouplingD cd;
+  cd.eps = c.eps;
+  cd.K = c.K;
+  cd.g = c.g;
+  return cd;
+}
+
 bool same_coupling(const Coupling& a, const Coupling& b) {
   return std::memcmp(&a, &b, sizeof(Coupling)) == 0;
 }
@@ -315,7 +323,7 @@ int set_control_impl(chll_lattice* L, double d, long long step, long long adapt_
   return CHLL_OK;
 }
 
-int observe_impl(chll_lattice* L, const Coupling& cp, double* dev_row, long long step) {
+int observe_impl(chll_lattice* L, const chll::CouplingD& cp, double* dev_row, long long step) {
   chll::launch_observables(L->view(), cp, L->ctl, L->partials, &L->tickets[0], dev_row, step,
                            L->stream);
   CHLL_CUDA_TRY(cudaGetLastError());
@@ -340,6 +348,7 @@ int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out) {
   if (n >= (1LL << 32) || groups >= (1LL << 32))
     return fail(CHLL_EINVAL, "lattice too large for 32-bit random counters (%lld sites)", n);
   CHLL_TRY(check_device());
+  chll::sweep_prepare();
 
   chll_lattice* L = new chll_lattice();
   L->ni = ni;
@@ -473,7 +482,7 @@ int run_impl(const chll_run_config& cfg, int nstart, int nstop, int nout, double
     if (end == meas) {
       if (r < rows) {
         double* drow = L->rows + r * chll::kRowLen;
-        rc = observe_impl(L, cp, drow, end);
+        rc = observe_impl(L, make_coupling_d(cc), drow, end);
         if (rc != CHLL_OK) break;
         cudaEvent_t ev;
         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -765,7 +774,7 @@ int chll_lattice_measure(chll_lattice* L, const chll_coupling* c, int slot) {
   if (!L || !c) return fail(CHLL_EINVAL, "measure: null argument");
   if (slot < 0 || slot >= L->rows_cap)
     return fail(CHLL_ERANGE, "measure: row %d outside the %d reserved rows", slot, L->rows_cap);
-  CHLL_TRY(observe_impl(L, make_coupling(*c), L->rows + (size_t)slot * chll::kRowLen, -1));
+  CHLL_TRY(observe_impl(L, make_coupling_d(*c), L->rows + (size_t)slot * chll::kRowLen, -1));
   return ok();
 }
 
@@ -787,7 +796,7 @@ int chll_lattice_observe(chll_lattice* L, const chll_coupling* c, double* row16)
   Control ctl;
   CHLL_CUDA_TRY(cudaMemcpyAsync(&ctl, L->ctl, sizeof(ctl), cudaMemcpyDeviceToHost, L->stream));
   CHLL_CUDA_TRY(cudaStreamSynchronize(L->stream));
-  CHLL_TRY(observe_impl(L, make_coupling(*c), drow, ctl.step - 1));
+  CHLL_TRY(observe_impl(L, make_coupling_d(*c), drow, ctl.step - 1));
   CHLL_CUDA_TRY(cudaMemcpyAsync(row16, drow, sizeof(double) * chll::kRowLen,
                                 cudaMemcpyDeviceToHost, L->stream));
   CHLL_CUDA_TRY(cudaStreamSynchronize(L->stream));
@@ -799,7 +808,7 @@ int chll_lattice_energy_grad(chll_lattice* L, const chll_coupling* c, float* gra
   if (!L || !c) return fail(CHLL_EINVAL, "energy_grad: null argument");
   const size_t total = 2 * L->per_colour;
   if (grad && !L->grad) CHLL_CUDA_TRY(cudaMalloc(&L->grad, total * sizeof(float4)));
-  chll::launch_energy_grad(L->view(), make_coupling(*c), grad ? L->grad : nullptr, project,
+  chll::launch_energy_grad(L->view(), make_coupling_d(*c), grad ? L->grad : nullptr, project,
                            L->partials, &L->tickets[1], L->out4, L->stream);
   CHLL_CUDA_TRY(cudaGetLastError());
   if (grad) {

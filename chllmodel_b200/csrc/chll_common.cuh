@@ -79,11 +79,39 @@ struct LatticeView {
 
 __host__ __device__ __forceinline__ int padded_ni(int ni) { return (ni + 3) & ~3; }
 
+// Division of x < 2^31 by a fixed divisor d >= 1 as one 32x32->64 multiply
+// and a shift: with s = ceil(log2 d), m = ceil(2^(31+s)/d) < 2^32 and
+// x*m = x*2^(31+s)/d + x*e/d (0 <= e < d), the error term is below
+// 2^31*d/(d*2^(31+s)) = 2^-s <= 1/d, so floor(x*m / 2^(31+s)) = floor(x/d)
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994).
+struct FastDiv {
+  uint32_t d, m, shift;  // shift = 31 + s
+
+  __host__ __device__ FastDiv() : d(1), m(0x80000000u), shift(31) {}
+  __host__ explicit FastDiv(uint32_t divisor) : d(divisor) {
+    uint32_t s = 0;
+    while ((1ull << s) < divisor) ++s;
+    shift = 31 + s;
+    const unsigned __int128 num = (unsigned __int128)1 << shift;
+    m = (uint32_t)((num + divisor - 1) / divisor);
+  }
+  __host__ __device__ __forceinline__ uint32_t div(uint32_t x) const {
+    return (uint32_t)(((uint64_t)x * m) >> shift);
+  }
+};
+
 struct Coupling {
   float eps;     // nematic coupling (reference: 1)
   float K;       // chiral coupling KK
   float g;       // field on the chirality
   float inv_kT;  // 1/kT (+inf at kT = 0, as the reference's division gives)
+};
+
+// Couplings in FP64 for the FP64 observables and adjoint sums, so that a
+// coupling such as eps = 1.2 enters those sums unrounded.
+struct CouplingD {
+  double eps, K, g;
 };
 
 // Per-replica control block, resident in device memory so that graph-captured

@@ -25,10 +25,15 @@ __device__ __forceinline__ float cross_axis(float vx, float vy, float vz, float4
 // Director proposal of chll_mod.f90:149-182: rotate n in its tangent plane by
 // amplitude d at angle phi = 2*pi*u, then renormalise.  |nz| > 0.999 (FP64 in
 // the reference) is exactly |nz| >= 0.999f for an FP32 nz.
+// The angle is taken as psi = 2*pi*(u - 1/2) in [-pi, pi), where the hardware
+// sine/cosine have absolute error <= 2^-21.4, and sin(phi) = -sin(psi),
+// cos(phi) = -cos(psi); u - 1/2 is exact for a 24-bit uniform.
 __device__ __forceinline__ void propose_director(float nx, float ny, float nz, float d, float u,
                                                  float& mx, float& my, float& mz) {
   float sn, cs;
-  sincospif(2.0f * u, &sn, &cs);
+  __sincosf(6.28318530717958647692f * (u - 0.5f), &sn, &cs);
+  sn = -sn;
+  cs = -cs;
   float x, y, z;
   if (fabsf(nz) >= 0.999f) {
     x = nx + d * cs;
@@ -104,7 +109,7 @@ __device__ __forceinline__ float spin_dE(const float4& n, const Nbrs& nb, const 
 // u <= exp(-dE/kT).  At kT = 0 this gives exp(-inf) = 0 for dE > 0 and NaN
 // (reject) for dE = 0, as the reference's division does.
 __device__ __forceinline__ bool metropolis(float dE, float u, float inv_kT) {
-  return (dE < 0.f) || (u <= expf(-dE * inv_kT));
+  return (dE < 0.f) || (u <= __expf(-dE * inv_kT));
 }
 
 }  // namespace chll

@@ -148,11 +148,10 @@ extern "C" int chll_energy_grad_noalloc(const void* colour0, const void* colour1
   v.nk = nk;
   v.hx = hx;
   v.periodic = boundary;
-  chll::Coupling cp;
-  cp.eps = (float)c->eps;
-  cp.K = (float)c->K;
-  cp.g = (float)c->g;
-  cp.inv_kT = (float)(1.0 / c->kT);
+  chll::CouplingD cp;
+  cp.eps = c->eps;
+  cp.K = c->K;
+  cp.g = c->g;
   chll::launch_energy_grad(v, cp, grad ? grad_rb : nullptr, project, partials, ticket, out4, s);
   if (grad) {
     chll::LatticeView gv = v;

@@ -35,7 +35,7 @@ __device__ __forceinline__ double fwd_bond(double eps, double K, double dot, dou
 }
 
 __global__ void __launch_bounds__(kObsThreads)
-    observables_kernel(LatticeView L, Coupling cp, const Control* __restrict__ ctl,
+    observables_kernel(LatticeView L, CouplingD cp, const Control* __restrict__ ctl,
                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
                        double* __restrict__ row, long long step) {
   const double eps = cp.eps, K = cp.K, g = cp.g;
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kObsThreads)
 
 int observables_max_blocks() { return kObsMaxBlocks; }
 
-void launch_observables(const LatticeView& L, const Coupling& cp, const Control* ctl,
+void launch_observables(const LatticeView& L, const CouplingD& cp, const Control* ctl,
                         double* partials, unsigned int* ticket, double* row, long long step,
                         cudaStream_t stream) {
   const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;

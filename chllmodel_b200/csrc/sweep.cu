@@ -2,15 +2,24 @@
 //
 // One launch is one of the reference's four half-sweeps per step
 // (chll_mod.f90:70,74,78,81): director trials on colour 0, on colour 1, then
-// chirality flips on colour 0, on colour 1.  Each thread owns the two
-// same-colour sites of one 4-site x-block (storage slots 2q, 2q+1 of a row),
-// draws both sites' randoms from a single Philox call keyed on the block, and
-// stores the pair back with two coalesced 128-bit stores.
+// chirality flips on colour 0, on colour 1.
 //
-// Accept counts are warp-aggregated and added once per CTA; the last CTA to
-// finish a pass (ticket counter) runs the step epilogue of chll_mod.f90:83-93
-// on the device: paccept and the d adaptation after the second director pass,
-// faccept and the step increment after the second flip pass.
+// Work unit: the two same-colour sites of one 4-site x-block (storage slots
+// 2q, 2q+1 of a row).  A thread draws both sites' randoms from a single
+// Philox call keyed on the block and stores the pair back with two coalesced
+// 128-bit stores.  Units are numbered row-major (g = q + Q*row) and CTAs walk
+// them grid-stride, so a launch is a few CTAs per SM that stay resident for
+// the whole pass: accept counts stay in registers and the CTA-wide reduction,
+// the one atomic and the completion ticket happen once per CTA.  All index
+// arithmetic is 32-bit (per-colour arrays < 2^31 slots); the row and plane
+// of a unit come from multiply-shift divisions.
+//
+// The last CTA to finish a pass (ticket counter) runs the step epilogue of
+// chll_mod.f90:83-93 on the device: paccept and the d adaptation after the
+// second director pass, faccept and the step increment after the second flip
+// pass.
+#include <mutex>
+
 #include "chll_common.cuh"
 #include "chll_physics.cuh"
 #include "sweep.cuh"
@@ -19,86 +28,84 @@ namespace chll {
 
 namespace {
 
+constexpr int kThreads = 256;
+
+struct SweepGeom {
+  uint32_t Q;        // units (4-site blocks) per row = hx/2
+  uint32_t units;    // Q * nj * nk
+  FastDiv by_Q;      // unit -> row
+  FastDiv by_nj;     // row -> plane
+};
+
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
-// Loads the six neighbours of site i (row j,k) from the other colour array.
-// hb: storage slot of this site's y/z neighbours (same h in the adjacent rows).
-__device__ __forceinline__ void load_yz(const float4* __restrict__ oth, const LatticeView& L,
-                                        int j, int k, int h, Nbrs& nb, bool have_jm,
-                                        bool have_jp, bool have_km, bool have_kp, int jm, int jp,
-                                        int km, int kp) {
-  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-  nb.b[2] = have_jp ? ld4(oth + ((size_t)k * L.nj + jp) * L.hx + h) : z;
-  nb.b[3] = have_jm ? ld4(oth + ((size_t)k * L.nj + jm) * L.hx + h) : z;
-  nb.b[4] = have_kp ? ld4(oth + ((size_t)kp * L.nj + j) * L.hx + h) : z;
-  nb.b[5] = have_km ? ld4(oth + ((size_t)km * L.nj + j) * L.hx + h) : z;
-}
-
-}  // namespace
-
 template <bool DIRECTOR, int C>
-__global__ void __launch_bounds__(256) sweep_pass_kernel(LatticeView L, Coupling cp, uint32_t key0,
-                                                         uint32_t key1, uint32_t replica,
-                                                         Control* __restrict__ ctl) {
+__global__ void __launch_bounds__(kThreads, 3)
+    sweep_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, uint32_t key0, uint32_t key1,
+                      uint32_t replica, Control* __restrict__ ctl) {
   constexpr uint32_t kPass = (DIRECTOR ? 0u : 2u) + (uint32_t)C;
-  const int Q = L.hx >> 1;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
   const long long step = ctl->step;
   const float d = (float)ctl->d;
+  const uint32_t hx = (uint32_t)L.hx;
+  const uint32_t nj = (uint32_t)L.nj, nk = (uint32_t)L.nk, ni = (uint32_t)L.ni;
+  const uint32_t plane = hx * nj;  // slots per plane
+  float4* __restrict__ cen_base = L.col[C];
+  const float4* __restrict__ oth = L.col[C ^ 1];
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
 
   unsigned int accepted = 0;
-  if (q < Q && j < L.nj) {
-    const int o = (C + j + k) & 1;
-    const int i0 = 4 * q + o;
-    const int i1 = i0 + 2;
-    const bool v0 = i0 < L.ni;
-    const bool v1 = i1 < L.ni;
-    const size_t row = (size_t)k * L.nj + j;
-    float4* __restrict__ cen = L.col[C] + row * L.hx + 2 * q;
-    const float4* __restrict__ oth = L.col[C ^ 1];
-    const float4* __restrict__ orow = oth + row * L.hx;
+  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
+       g += gridDim.x * kThreads) {
+    const uint32_t row = G.by_Q.div(g);
+    const uint32_t q = g - row * G.Q;
+    const uint32_t k = G.by_nj.div(row);
+    const uint32_t j = row - k * nj;
+    const uint32_t o = (C + j + k) & 1u;
+    const uint32_t i0 = 4 * q + o;
+    const uint32_t i1 = i0 + 2;
+    const bool v0 = i0 < ni;
+    const bool v1 = i1 < ni;
+    const uint32_t rs = row * hx;  // slot of the row start
+    float4* cen = cen_base + rs + 2 * q;
     float4 n0 = cen[0];
     float4 n1 = cen[1];
 
-    int jm = j - 1, jp = j + 1, km = k - 1, kp = k + 1;
-    bool hjm = true, hjp = true, hkm = true, hkp = true;
-    // x neighbours: xa = i0-1, xb = i0+1 = i1-1, xc = i1+1.
-    int xa = i0 - 1, xb = i0 + 1, xc = i1 + 1;
-    bool hxa = true, hxb = true, hxc = true;
+    // neighbour rows (slot offsets) and their presence
+    uint32_t sjm = rs - hx, sjp = rs + hx, skm = rs - plane, skp = rs + plane;
+    bool hjm = j > 0, hjp = j + 1 < nj, hkm = k > 0, hkp = k + 1 < nk;
+    // x neighbours of i0 and i1: xa = i0-1, xb = i0+1 = i1-1, xc = i1+1
+    uint32_t xa = i0 - 1, xb = i0 + 1, xc = i1 + 1;
+    bool hxa = i0 > 0, hxb = xb < ni, hxc = xc < ni;
     if (L.periodic) {
-      if (jm < 0) jm = L.nj - 1;
-      if (jp >= L.nj) jp = 0;
-      if (km < 0) km = L.nk - 1;
-      if (kp >= L.nk) kp = 0;
-      if (xa < 0) xa = L.ni - 1;
-      if (xb >= L.ni) xb = 0;
-      if (xc >= L.ni) xc = 0;
-    } else {
-      hjm = jm >= 0;
-      hjp = jp < L.nj;
-      hkm = km >= 0;
-      hkp = kp < L.nk;
-      hxa = xa >= 0;
-      hxb = xb < L.ni;
-      hxc = xc < L.ni;
+      if (!hjm) sjm = rs + (nj - 1) * hx;
+      if (!hjp) sjp = rs - (nj - 1) * hx;
+      if (!hkm) skm = rs + (nk - 1) * plane;
+      if (!hkp) skp = rs - (nk - 1) * plane;
+      if (!hxa) xa = ni - 1;
+      if (!hxb) xb = 0;
+      if (!hxc) xc = 0;
+      hjm = hjp = hkm = hkp = hxa = hxb = hxc = true;
     }
-    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* orow = oth + rs;
     const float4 fa = hxa ? ld4(orow + (xa >> 1)) : zero;
     const float4 fb = hxb ? ld4(orow + (xb >> 1)) : zero;
     const float4 fc = hxc ? ld4(orow + (xc >> 1)) : zero;
-
+    const uint32_t h0 = 2 * q;
     Nbrs nb0, nb1;
     nb0.b[0] = fb;  // +x of i0
     nb0.b[1] = fa;  // -x of i0
     nb1.b[0] = fc;  // +x of i1
     nb1.b[1] = fb;  // -x of i1
-    load_yz(oth, L, j, k, 2 * q, nb0, hjm, hjp, hkm, hkp, jm, jp, km, kp);
-    load_yz(oth, L, j, k, 2 * q + 1, nb1, hjm, hjp, hkm, hkp, jm, jp, km, kp);
+    nb0.b[2] = hjp ? ld4(oth + sjp + h0) : zero;
+    nb1.b[2] = hjp ? ld4(oth + sjp + h0 + 1) : zero;
+    nb0.b[3] = hjm ? ld4(oth + sjm + h0) : zero;
+    nb1.b[3] = hjm ? ld4(oth + sjm + h0 + 1) : zero;
+    nb0.b[4] = hkp ? ld4(oth + skp + h0) : zero;
+    nb1.b[4] = hkp ? ld4(oth + skp + h0 + 1) : zero;
+    nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
+    nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
 
-    const uint32_t group = (uint32_t)(q + (size_t)Q * row);
-    Ctr4 ctr = {{group, (uint32_t)step, replica, kPass}};
+    Ctr4 ctr = {{g, (uint32_t)step, replica, kPass}};
     const Ctr4 r = philox4x32_10(ctr, key0, key1);
 
     if (DIRECTOR) {
@@ -144,10 +151,10 @@ __global__ void __launch_bounds__(256) sweep_pass_kernel(LatticeView L, Coupling
     cen[1] = n1;
   }
 
-  // Block-aggregated accept count, then the last-CTA epilogue.
+  // CTA-aggregated accept count, then the last-CTA epilogue.
   __shared__ unsigned int s_cnt;
   __shared__ bool s_last;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x;
   if (tid == 0) s_cnt = 0;
   __syncthreads();
   const unsigned int wsum = __reduce_add_sync(0xffffffffu, accepted);
@@ -157,9 +164,8 @@ __global__ void __launch_bounds__(256) sweep_pass_kernel(LatticeView L, Coupling
     unsigned long long* counter = DIRECTOR ? &ctl->nacc : &ctl->nflip;
     if (s_cnt) atomicAdd(counter, (unsigned long long)s_cnt);
     __threadfence();
-    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
     const unsigned int ticket = atomicAdd(&ctl->done, 1u);
-    s_last = (ticket == nblocks - 1);
+    s_last = (ticket == gridDim.x - 1);
   }
   __syncthreads();
   if (s_last && tid == 0) {
@@ -195,23 +201,68 @@ __global__ void __launch_bounds__(256) sweep_pass_kernel(LatticeView L, Coupling
   }
 }
 
+// Resident CTAs per SM of each pass kernel and the SM count, queried once
+// per device (outside any stream capture; see sweep_prepare).
+struct DeviceShape {
+  int sms = 0;
+  int per_sm[4] = {0, 0, 0, 0};
+};
+std::mutex g_shape_mutex;
+DeviceShape g_shape[64];
+
+template <bool D, int C>
+int occupancy() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_pass_kernel<D, C>, kThreads, 0);
+  return n > 0 ? n : 1;
+}
+
+const DeviceShape& device_shape() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lk(g_shape_mutex);
+  DeviceShape& s = g_shape[dev];
+  if (s.sms == 0) {
+    cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (s.sms <= 0) s.sms = 148;
+    s.per_sm[0] = occupancy<true, 0>();
+    s.per_sm[1] = occupancy<true, 1>();
+    s.per_sm[2] = occupancy<false, 0>();
+    s.per_sm[3] = occupancy<false, 1>();
+  }
+  return s;
+}
+
+}  // namespace
+
+void sweep_prepare() { (void)device_shape(); }
+
 void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int pass, cudaStream_t stream) {
-  const int Q = L.hx >> 1;
-  const dim3 block(32, 8, 1);
-  const dim3 grid((Q + 31) / 32, (L.nj + 7) / 8, L.nk);
+  const DeviceShape& ds = device_shape();
+  SweepGeom G;
+  G.Q = (uint32_t)(L.hx >> 1);
+  G.units = G.Q * (uint32_t)L.nj * (uint32_t)L.nk;
+  G.by_Q = FastDiv(G.Q);
+  G.by_nj = FastDiv((uint32_t)L.nj);
+  const uint32_t need = (G.units + kThreads - 1) / kThreads;
+  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.per_sm[pass & 3];
+  const dim3 grid(need < resident ? (need ? need : 1) : resident);
   switch (pass) {
     case kPassDir0:
-      sweep_pass_kernel<true, 0><<<grid, block, 0, stream>>>(L, cp, key0, key1, replica, ctl);
+      sweep_pass_kernel<true, 0><<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
       break;
     case kPassDir1:
-      sweep_pass_kernel<true, 1><<<grid, block, 0, stream>>>(L, cp, key0, key1, replica, ctl);
+      sweep_pass_kernel<true, 1><<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
       break;
     case kPassSpin0:
-      sweep_pass_kernel<false, 0><<<grid, block, 0, stream>>>(L, cp, key0, key1, replica, ctl);
+      sweep_pass_kernel<false, 0><<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica,
+                                                                 ctl);
       break;
     default:
-      sweep_pass_kernel<false, 1><<<grid, block, 0, stream>>>(L, cp, key0, key1, replica, ctl);
+      sweep_pass_kernel<false, 1><<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica,
+                                                                 ctl);
       break;
   }
 }

@@ -6,7 +6,9 @@
 
 namespace chll {
 
-// sweep.cu: one half-sweep (pass = kPassDir0..kPassSpin1).
+// sweep.cu: per-device launch shapes (call once per device, outside any
+// stream capture) and one half-sweep (pass = kPassDir0..kPassSpin1).
+void sweep_prepare();
 void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int pass, cudaStream_t stream);
 
@@ -22,12 +24,12 @@ void launch_init_random(const LatticeView& L, uint32_t key0, uint32_t key1, uint
 
 // observables.cu: FP64 moments and the measurement row.
 int observables_max_blocks();
-void launch_observables(const LatticeView& L, const Coupling& cp, const Control* ctl,
+void launch_observables(const LatticeView& L, const CouplingD& cp, const Control* ctl,
                         double* partials, unsigned int* ticket, double* row, long long step,
                         cudaStream_t stream);
 
 // adjoint.cu: energy gradient.
-void launch_energy_grad(const LatticeView& L, const Coupling& cp, float4* grad_rb, int project,
+void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,
                         double* partials, unsigned int* ticket, double* out4,
                         cudaStream_t stream);
 int energy_grad_max_blocks();
