@@ -289,6 +289,10 @@ def gpu_arm(args):
                                      "arrays, upload + pack + sweeps + measurements + unpack + "
                                      "download"}
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_vs_plain(args, rank, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(args.cpu_seconds)
@@ -319,12 +323,86 @@ def gpu_arm(args):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk,
+        "batched": batched,
         "final_control": ctl,
         "last_row": {"energy_per_site": float(rows[-1][5] / n) if len(rows) else None,
                      "eta": float(rows[-1][1]) if len(rows) else None},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batched_vs_plain(args, rank, torch):
+    """Phase-diagram grid: 64 replicas (kT on 8 points in 0.1-2.0 x h on 8 points
+    in 0.0-3.0, K=1, edges drawn from {32, 48, 64}, seed 1 + replica) for
+    `batched_sweeps` sweeps with FP64 measurements every 10 sweeps, as one
+    persistent launch versus the same points run one after another with the
+    plain kernels (graph-captured 10-sweep chunks + a measurement each)."""
+    import numpy as np
+
+    from chllmodel_b200.batched import Batch, phase_grid
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    nsw = args.batched_sweeps
+    specs = phase_grid(np.linspace(0.1, 2.0, 8), np.linspace(0.0, 3.0, 8), [32, 48, 64],
+                       K=1.0, seed=1 + 1000 * rank, size_seed=12345)
+    stream = torch.cuda.Stream()
+    b = Batch(specs)
+    b.set_stream(stream.cuda_stream)
+    b.init_random()
+    tune = b.autotune(trial_sweeps=20)
+    b.run(nsw, measure_every=10)   # warm-up: graph capture and first launch
+    b.sync()
+    b.close()
+    b = Batch(specs)
+    b.set_stream(stream.cuda_stream)
+    b.init_random()
+    b.set_tuning(tune["threads"], tune["ctas_per_sm"])
+    b.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.run(nsw, measure_every=10)
+    e1.record(stream)
+    e1.synchronize()
+    t_batched = e0.elapsed_time(e1) * 1e-3
+    summ = b.summary()
+    info = b.info()
+    b.close()
+
+    t_plain = 0.0
+    for sp in specs:
+        lat = Lattice(sp["ni"], sp["nj"], sp["nk"], boundary=sp["boundary"])
+        lat.set_stream(stream.cuda_stream)
+        lat.init_random(sp["seed"], sp["replica"])
+        lat.set_control(sp["d"], step=1)
+        lat.reserve_rows(nsw // 10 + 1)
+        cp = coupling(sp["kT"], sp["K"], sp["g"], sp["eps"])
+        lat.sweep(cp, 10, seed=sp["seed"], replica=sp["replica"])  # capture the graph
+        lat.sync()
+        lat.init_random(sp["seed"], sp["replica"])
+        lat.set_control(sp["d"], step=1)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for c in range(nsw // 10):
+            lat.sweep(cp, 10, seed=sp["seed"], replica=sp["replica"])
+            lat.measure(cp, c)
+        a1.record(stream)
+        a1.synchronize()
+        t_plain += a0.elapsed_time(a1) * 1e-3
+        lat.close()
+    total = info["total_sites"]
+    return {"workload": "64 replicas, edges {32,48,64}^3, kT x h grid 8x8, K=1, "
+                        f"{nsw} sweeps, FP64 measurements every 10 sweeps",
+            "replicas": len(specs), "total_sites": total, "sweeps": nsw,
+            "time_to_grid_s": t_batched, "sequential_plain_s": t_plain,
+            "speedup_vs_sequential_plain": t_plain / t_batched,
+            "site_updates_per_s": total * nsw / t_batched,
+            "tuning": {k: tune[k] for k in ("threads", "ctas_per_sm", "trial_ms")},
+            "grid_ctas": info["grid"],
+            "mean_S_lowest_kT": float(np.mean([r["S"] for r in summ if r["kT"] < 0.2])),
+            "mean_S_highest_kT": float(np.mean([r["S"] for r in summ if r["kT"] > 1.9]))}
 
 
 def main():
@@ -335,6 +413,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-sweeps", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--edge", type=int, default=L_EDGE,
                     help="lattice edge (480 is the benchmark; smaller edges for profiling)")

@@ -31,6 +31,9 @@ EXPORTS = (
     "chll_lattice_sweep", "chll_lattice_pass", "chll_lattice_observe",
     "chll_lattice_energy_grad", "chll_lattice_reserve_rows", "chll_lattice_measure",
     "chll_lattice_read_rows", "chll_energy_grad_noalloc",
+    "chll_batch_create", "chll_batch_destroy", "chll_batch_set_stream", "chll_batch_sync",
+    "chll_batch_init_random", "chll_batch_upload_f4", "chll_batch_download_f4", "chll_batch_run",
+    "chll_batch_moments", "chll_batch_info", "chll_batch_set_tuning", "chll_batch_autotune",
 )
 
 
@@ -147,25 +150,25 @@ def _declare(L: ct.CDLL) -> None:
     L.chll_energy_grad_noalloc.argtypes = [vp, vp, i32, i32, i32, i32, P(Coupling), i32, vp, vp,
                                            vp]
     L.chll_energy_grad_noalloc.restype = i32
-    if hasattr(L, "chll_batch_create"):
-        L.chll_batch_create.argtypes = [P(ReplicaSpec), i32, P(vp)]
-        L.chll_batch_create.restype = i32
-        L.chll_batch_destroy.argtypes = [vp]
-        L.chll_batch_destroy.restype = None
-        L.chll_batch_set_stream.argtypes = [vp, vp]
-        L.chll_batch_set_stream.restype = i32
-        L.chll_batch_run.argtypes = [vp, i32, i32, i32]
-        L.chll_batch_run.restype = i32
-        L.chll_batch_moments.argtypes = [vp, vp]
-        L.chll_batch_moments.restype = i32
-        L.chll_batch_download_f4.argtypes = [vp, i32, vp]
-        L.chll_batch_download_f4.restype = i32
-        L.chll_batch_upload_f4.argtypes = [vp, i32, vp]
-        L.chll_batch_upload_f4.restype = i32
-        L.chll_batch_info.argtypes = [vp, P(i64), P(i32), P(i32), P(i32)]
-        L.chll_batch_info.restype = i32
-        L.chll_batch_set_tuning.argtypes = [vp, i32, i32]
-        L.chll_batch_set_tuning.restype = i32
+    L.chll_batch_create.argtypes = [P(ReplicaSpec), i32, P(vp)]
+    L.chll_batch_create.restype = i32
+    L.chll_batch_destroy.argtypes = [vp]
+    L.chll_batch_destroy.restype = None
+    L.chll_batch_set_stream.argtypes = [vp, vp]
+    L.chll_batch_sync.argtypes = [vp]
+    L.chll_batch_init_random.argtypes = [vp]
+    L.chll_batch_run.argtypes = [vp, i32, i32, i32]
+    L.chll_batch_moments.argtypes = [vp, vp]
+    L.chll_batch_download_f4.argtypes = [vp, i32, vp]
+    L.chll_batch_upload_f4.argtypes = [vp, i32, vp]
+    L.chll_batch_info.argtypes = [vp, P(i64), P(ct.c_int32), P(ct.c_int32), P(ct.c_int32)]
+    L.chll_batch_set_tuning.argtypes = [vp, i32, i32]
+    L.chll_batch_autotune.argtypes = [vp, i32, P(i32), P(i32), P(dbl)]
+    for name in ("chll_batch_set_stream", "chll_batch_sync", "chll_batch_init_random",
+                 "chll_batch_run", "chll_batch_moments", "chll_batch_download_f4",
+                 "chll_batch_upload_f4", "chll_batch_info", "chll_batch_set_tuning",
+                 "chll_batch_autotune"):
+        getattr(L, name).restype = i32
 
 
 def check(rc: int) -> None:

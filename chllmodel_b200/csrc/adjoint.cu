@@ -23,7 +23,7 @@ constexpr int kGradThreads = 256;
 constexpr int kGradMaxBlocks = 148 * 4;
 
 __device__ __forceinline__ float4 site(const LatticeView& L, int i, int j, int k) {
-  return L.col[(i + j + k) & 1][((size_t)k * L.nj + j) * L.hx + (i >> 1)];
+  return colour_array(L, (i + j + k) & 1)[((size_t)k * L.nj + j) * L.hx + (i >> 1)];
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kGradThreads)
       if (grad_rb) grad_rb[e] = zero;
       continue;
     }
-    const float4 n = L.col[col][t];
+    const float4 n = colour_array(L, col)[t];
     int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
     bool hip = ip < L.ni, him = im >= 0, hjp = jp < L.nj, hjm = jm >= 0, hkp = kp < L.nk,
          hkm = km >= 0;

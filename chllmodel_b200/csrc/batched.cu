@@ -1,0 +1,790 @@
+// Batched replicas: many independent lattices of uneven size, each with its
+// own (kT, h, K, eps, seed, d), swept for a fixed number of steps and
+// measured in FP64 inside ONE persistent cooperative launch.
+//
+// This replaces the reference's phase-diagram workflow of one process and
+// one ChLLSim per (kT, K, g) point (e.g. scripts/phase_diagram.py:24-31,
+// scripts/g_field0.5.py:24-31).
+//
+// Layout: each replica keeps the plain lattice layout (two red/black float4
+// colour arrays) in one shared allocation, and a ReplicaState block holds its
+// d, step, accept counters, barrier words and FP64 measurement accumulators.
+//
+// Schedule: the launch is sized to the co-resident CTA count (cooperative
+// launch), and every replica owns a contiguous group of CTAs proportional to
+// its number of sites (at least one).  A group walks its replica's units
+// grid-stride with the same sweep_unit() as the plain kernel, so a replica's
+// chain is bit-identical to the same replica run alone.  Between half-sweeps
+// the group meets at a software barrier in global memory (arrive counter +
+// generation word).  Every wait is bounded: on timeout the CTA sets the
+// replica's status word and returns, and so do the others at their next
+// barrier, so a fault ends the launch instead of hanging it.
+//
+// Measurements every `measure_every` sweeps (from sweep `measure_from`):
+// per-CTA FP64 moments (moments.cuh) -> partial slots -> the group's first
+// CTA sums them in a fixed order and accumulates e = E/N, eta = sum(s)/N and
+// the nematic order S = largest eigenvalue of Q = (3/2)<n n^T> - I/2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/chll_mod.h"
+#include "chll_common.cuh"
+#include "moments.cuh"
+#include "sweep.cuh"
+#include "sweep_unit.cuh"
+
+namespace chll {
+int record_error(int code, const char* msg);
+int record_ok();
+}  // namespace chll
+
+namespace chll {
+namespace {
+
+struct ReplicaDesc {
+  LatticeView L;
+  SweepGeom G;
+  Coupling cp;
+  CouplingD cd;
+  uint32_t key0, key1, replica;
+  int cta_first, cta_count;
+  long long nsites;
+  long long adapt_until;
+};
+
+struct ReplicaState {
+  double d;
+  long long step;
+  unsigned long long cnt[4];  // director counts by sweep parity [0,1], flips [2,3]
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  unsigned int status;
+  unsigned int pad;
+  float paccept, faccept;
+  double mom[8];   // n, sum e, sum e^2, sum eta, sum eta^2, sum |eta|, sum S, sum S^2
+  double last[3];  // last e, eta, S
+};
+
+constexpr int kMomLen = 16;  // chll_batch_moments row
+
+// Largest eigenvalue of a symmetric 3x3 matrix (Smith, "Eigenvalues of a
+// symmetric 3x3 matrix", CACM 4(4):168, 1961): trigonometric solution of the
+// characteristic cubic.
+__host__ __device__ inline double sym3_max_eig(double a11, double a22, double a33, double a12,
+                                               double a13, double a23) {
+  const double p1 = a12 * a12 + a13 * a13 + a23 * a23;
+  const double q = (a11 + a22 + a33) / 3.0;
+  const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
+  const double p2 = b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * p1;
+  if (p2 <= 0.0) return q;
+  const double p = sqrt(p2 / 6.0);
+  const double c11 = b11 / p, c22 = b22 / p, c33 = b33 / p;
+  const double c12 = a12 / p, c13 = a13 / p, c23 = a23 / p;
+  const double det = c11 * (c22 * c33 - c23 * c23) - c12 * (c12 * c33 - c23 * c13) +
+                     c13 * (c12 * c23 - c22 * c13);
+  double r = det / 2.0;
+  r = r < -1.0 ? -1.0 : (r > 1.0 ? 1.0 : r);
+  const double phi = acos(r) / 3.0;
+  return q + 2.0 * p * cos(phi);
+}
+
+// Group barrier of one replica's CTAs.  Returns false if the replica's status
+// word is set (a wait timed out here or in another CTA of the group).
+__device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limit) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* genp = &st->bar_gen;
+    volatile unsigned int* statp = &st->status;
+    int ok = 1;
+    if (nct > 1) {
+      const unsigned int gen = *genp;
+      __threadfence();
+      const unsigned int arrived = atomicAdd(&st->bar_count, 1u);
+      if (arrived == (unsigned int)nct - 1) {
+        st->bar_count = 0;
+        __threadfence();
+        atomicAdd(&st->bar_gen, 1u);
+      } else {
+        unsigned long long it = 0;
+        while (*genp == gen) {
+          if (*statp) break;
+          if (++it > limit) {
+            atomicOr(&st->status, 1u);
+            break;
+          }
+          __nanosleep(100);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok && (*statp == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int THREADS>
+__device__ __forceinline__ unsigned int cta_sum(unsigned int v) {
+  __shared__ unsigned int s_w[THREADS / 32];
+  v = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned int t = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < THREADS / 32; ++w) t += s_w[w];
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+template <bool DIRECTOR, int C, int THREADS>
+__device__ __forceinline__ unsigned int group_pass(const ReplicaDesc& D, int rank, uint32_t step,
+                                                   float d) {
+  unsigned int acc = 0;
+  const uint32_t stride = (uint32_t)D.cta_count * THREADS;
+  if (D.L.periodic) {
+    for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units; g += stride)
+      acc += sweep_unit<DIRECTOR, C, true>(D.L, D.G, g, step, d, D.cp, D.key0, D.key1,
+                                           D.replica);
+  } else {
+    for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units; g += stride)
+      acc += sweep_unit<DIRECTOR, C, false>(D.L, D.G, g, step, d, D.cp, D.key0, D.key1,
+                                            D.replica);
+  }
+  return acc;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 768 / THREADS)
+    batch_kernel(const ReplicaDesc* __restrict__ descs, ReplicaState* __restrict__ states,
+                 const int* __restrict__ cta_replica, double* __restrict__ partials,
+                 int nsweeps, int measure_every, int measure_from, unsigned long long limit) {
+  const int rep = cta_replica[blockIdx.x];
+  const ReplicaDesc D = descs[rep];
+  ReplicaState* st = states + rep;
+  const int rank = (int)blockIdx.x - D.cta_first;
+  const int nct = D.cta_count;
+  const float n3 = (float)D.nsites;
+  double d = st->d;
+  long long step = st->step;
+  __shared__ double s_d;
+
+  for (int s = 0; s < nsweeps; ++s, ++step) {
+    const uint32_t step32 = (uint32_t)step;
+    const int par = (int)(step & 1);
+    // director trials: colour 0, colour 1 (chll_mod.f90:70,74)
+    unsigned int acc = group_pass<true, 0, THREADS>(D, rank, step32, (float)d);
+    if (!group_barrier(st, nct, limit)) return;
+    acc += group_pass<true, 1, THREADS>(D, rank, step32, (float)d);
+    acc = cta_sum<THREADS>(acc);
+    if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[par], (unsigned long long)acc);
+    if (!group_barrier(st, nct, limit)) return;
+    // Every CTA of the group derives the same new d from the group's count
+    // (chll_mod.f90:83-90); the director count of the other parity is reset
+    // here for the next sweep (all CTAs finished reading it a sweep ago).
+    if (threadIdx.x == 0) {
+      const unsigned long long na = *((volatile unsigned long long*)&st->cnt[par]);
+      const float pa = (float)na / n3;
+      s_d = (step < D.adapt_until) ? adapt_d(d, pa) : d;
+      if (rank == 0) {
+        st->cnt[par ^ 1] = 0;
+        st->paccept = pa;
+      }
+    }
+    __syncthreads();
+    d = s_d;
+    // chirality flips: colour 0, colour 1 (chll_mod.f90:78,81)
+    acc = group_pass<false, 0, THREADS>(D, rank, step32, (float)d);
+    if (!group_barrier(st, nct, limit)) return;
+    acc += group_pass<false, 1, THREADS>(D, rank, step32, (float)d);
+    acc = cta_sum<THREADS>(acc);
+    if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[2 + par], (unsigned long long)acc);
+    if (!group_barrier(st, nct, limit)) return;
+    if (threadIdx.x == 0 && rank == 0) {
+      const unsigned long long nf = *((volatile unsigned long long*)&st->cnt[2 + par]);
+      st->faccept = (float)nf / n3;
+      st->cnt[2 + (par ^ 1)] = 0;
+    }
+
+    // FP64 measurement
+    const int done = s + 1;
+    if (measure_every > 0 && done >= measure_from && done % measure_every == 0) {
+      double m[kObsMoments];
+#pragma unroll
+      for (int t = 0; t < kObsMoments; ++t) m[t] = 0.0;
+      const size_t per_colour = (size_t)D.L.hx * D.L.nj * D.L.nk;
+      const size_t total = 2 * per_colour;
+      for (size_t e = (size_t)rank * THREADS + threadIdx.x; e < total;
+           e += (size_t)nct * THREADS)
+        site_moments(D.L, D.cd, e, per_colour, m);
+      __shared__ double s_m[THREADS / 32][kObsMoments];
+#pragma unroll
+      for (int t = 0; t < kObsMoments; ++t) {
+        const double v = warp_sum_d(m[t]);
+        if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5][t] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < kObsMoments) {
+        double v = 0.0;
+        for (int w = 0; w < THREADS / 32; ++w) v += s_m[w][threadIdx.x];
+        partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
+      }
+      if (!group_barrier(st, nct, limit)) return;
+      if (rank == 0 && threadIdx.x == 0) {
+        double tot[kObsMoments];
+        for (int t = 0; t < kObsMoments; ++t) tot[t] = 0.0;
+        for (int c = 0; c < nct; ++c)
+          for (int t = 0; t < kObsMoments; ++t)
+            tot[t] += *((volatile double*)&partials[(size_t)(D.cta_first + c) * kObsMoments + t]);
+        const double n = (double)D.nsites;
+        const double e = tot[0] / n, eta = tot[2] / n;
+        const double qxx = 1.5 * tot[3] / n - 0.5, qyy = 1.5 * tot[4] / n - 0.5,
+                     qzz = 1.5 * tot[5] / n - 0.5;
+        const double qxy = 1.5 * tot[6] / n, qxz = 1.5 * tot[7] / n, qyz = 1.5 * tot[8] / n;
+        const double S = sym3_max_eig(qxx, qyy, qzz, qxy, qxz, qyz);
+        st->mom[0] += 1.0;
+        st->mom[1] += e;
+        st->mom[2] += e * e;
+        st->mom[3] += eta;
+        st->mom[4] += eta * eta;
+        st->mom[5] += fabs(eta);
+        st->mom[6] += S;
+        st->mom[7] += S * S;
+        st->last[0] = e;
+        st->last[1] = eta;
+        st->last[2] = S;
+      }
+    }
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    st->d = d;
+    st->step = step;
+  }
+}
+
+}  // namespace
+}  // namespace chll
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace chll {
+namespace {
+
+using BatchKernel = void (*)(const ReplicaDesc*, ReplicaState*, const int*, double*, int, int, int,
+                             unsigned long long);
+
+BatchKernel kernel_for(int threads) {
+  switch (threads) {
+    case 128: return batch_kernel<128>;
+    case 512: return batch_kernel<512>;
+    default: return batch_kernel<256>;
+  }
+}
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return record_error(code, buf);
+}
+
+#define BATCH_CUDA(expr)                                                                      \
+  do {                                                                                        \
+    cudaError_t _e = (expr);                                                                  \
+    if (_e != cudaSuccess)                                                                    \
+      return fail(_e == cudaErrorMemoryAllocation ? CHLL_ENOMEM : CHLL_ECUDA, "%s: %s", #expr, \
+                  cudaGetErrorString(_e));                                                    \
+  } while (0)
+
+constexpr int kMaxCtasPerSm = 16;
+
+}  // namespace
+}  // namespace chll
+
+struct chll_batch {
+  int n = 0;
+  std::vector<chll_replica_spec> specs;
+  std::vector<chll::ReplicaDesc> desc;  // host copy, cta ranges filled per launch shape
+  std::vector<size_t> offset;           // first float4 slot of each replica
+  std::vector<size_t> per_colour;
+  float4* lat = nullptr;
+  size_t slots = 0;
+  chll::ReplicaDesc* d_desc = nullptr;
+  chll::ReplicaState* d_state = nullptr;
+  int* d_cta_replica = nullptr;
+  double* d_partials = nullptr;
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  float4* snap_lat = nullptr;
+  chll::ReplicaState* snap_state = nullptr;
+  cudaStream_t own_stream = nullptr, capture_stream = nullptr, stream = nullptr;
+  int sms = 148;
+  int threads = 256;
+  int ctas_per_sm = 0;  // 0: as many as fit
+  int grid = 0;         // CTAs of the current launch shape
+  int shape_threads = -1, shape_ctas = -1;
+  cudaGraphExec_t graph = nullptr;
+  int g_sweeps = -1, g_every = -1, g_from = -1, g_grid = -1, g_threads = -1;
+  unsigned long long limit = 1ull << 24;
+  long long total_sites = 0;
+
+  chll::LatticeView view(int r) const { return desc[r].L; }
+};
+
+namespace {
+
+using chll::fail;
+
+int occupancy_of(int threads) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, chll::kernel_for(threads), threads, 0);
+  return n;
+}
+
+// CTAs per replica proportional to its units, at least one each, at most one
+// per `threads` units; fills desc[].cta_first/cta_count and the CTA map.
+int shape_launch(chll_batch* B) {
+  if (B->shape_threads == B->threads && B->shape_ctas == B->ctas_per_sm && B->grid > 0)
+    return CHLL_OK;
+  const int occ = occupancy_of(B->threads);
+  if (occ <= 0) return fail(CHLL_ECUDA, "batch: kernel with %d threads cannot run", B->threads);
+  const int per_sm = std::min(B->ctas_per_sm > 0 ? std::min(B->ctas_per_sm, occ) : occ,
+                              chll::kMaxCtasPerSm);
+  const int budget = B->sms * per_sm;
+  if (B->n > budget)
+    return fail(CHLL_ERANGE,
+                "batch: %d replicas need at least %d co-resident CTAs; this shape holds %d",
+                B->n, B->n, budget);
+  std::vector<double> units(B->n);
+  double tot = 0.0;
+  for (int r = 0; r < B->n; ++r) {
+    units[r] = (double)B->desc[r].G.units;
+    tot += units[r];
+  }
+  std::vector<int> cnt(B->n, 1);
+  std::vector<int> cap(B->n);
+  for (int r = 0; r < B->n; ++r)
+    cap[r] = std::max(1, (int)((B->desc[r].G.units + B->threads - 1) / B->threads));
+  int used = B->n;
+  // largest remainder on the share of the remaining CTAs
+  const int extra = budget - B->n;
+  std::vector<std::pair<double, int>> rem;
+  for (int r = 0; r < B->n; ++r) {
+    const double want = extra * units[r] / tot;
+    const int add = std::min((int)want, cap[r] - 1);
+    cnt[r] += add;
+    used += add;
+    rem.push_back({want - (int)want, r});
+  }
+  std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
+  for (auto& pr : rem) {
+    if (used >= budget) break;
+    if (cnt[pr.second] < cap[pr.second]) {
+      ++cnt[pr.second];
+      ++used;
+    }
+  }
+  std::vector<int> map;
+  map.reserve(used);
+  for (int r = 0; r < B->n; ++r) {
+    B->desc[r].cta_first = (int)map.size();
+    B->desc[r].cta_count = cnt[r];
+    for (int c = 0; c < cnt[r]; ++c) map.push_back(r);
+  }
+  B->grid = (int)map.size();
+  if (B->d_cta_replica) cudaFree(B->d_cta_replica);
+  B->d_cta_replica = nullptr;
+  BATCH_CUDA(cudaMalloc(&B->d_cta_replica, sizeof(int) * map.size()));
+  BATCH_CUDA(cudaMemcpyAsync(B->d_cta_replica, map.data(), sizeof(int) * map.size(),
+                             cudaMemcpyHostToDevice, B->stream));
+  BATCH_CUDA(cudaMemcpyAsync(B->d_desc, B->desc.data(), sizeof(chll::ReplicaDesc) * B->n,
+                             cudaMemcpyHostToDevice, B->stream));
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  B->shape_threads = B->threads;
+  B->shape_ctas = B->ctas_per_sm;
+  return CHLL_OK;
+}
+
+int launch_batch(chll_batch* B, cudaStream_t s, int nsweeps, int every, int from) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)B->grid);
+  cfg.blockDim = dim3((unsigned)B->threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BATCH_CUDA(cudaLaunchKernelEx(&cfg, chll::kernel_for(B->threads),
+                                (const chll::ReplicaDesc*)B->d_desc, B->d_state,
+                                (const int*)B->d_cta_replica, B->d_partials, nsweeps, every, from,
+                                B->limit));
+  return CHLL_OK;
+}
+
+int run_impl(chll_batch* B, int nsweeps, int every, int from) {
+  int rc = shape_launch(B);
+  if (rc != CHLL_OK) return rc;
+  if (!(B->graph && B->g_sweeps == nsweeps && B->g_every == every && B->g_from == from &&
+        B->g_grid == B->grid && B->g_threads == B->threads)) {
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    BATCH_CUDA(cudaStreamBeginCapture(B->capture_stream, cudaStreamCaptureModeThreadLocal));
+    rc = launch_batch(B, B->capture_stream, nsweeps, every, from);
+    cudaError_t e = cudaStreamEndCapture(B->capture_stream, &g);
+    if (rc != CHLL_OK) return rc;
+    if (e != cudaSuccess) return fail(CHLL_ECUDA, "batch: capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CHLL_ECUDA, "batch: instantiate: %s", cudaGetErrorString(e));
+    B->g_sweeps = nsweeps;
+    B->g_every = every;
+    B->g_from = from;
+    B->g_grid = B->grid;
+    B->g_threads = B->threads;
+  }
+  BATCH_CUDA(cudaGraphLaunch(B->graph, B->stream));
+  return CHLL_OK;
+}
+
+int ensure_staging(chll_batch* B, size_t bytes) {
+  if (B->staging_bytes >= bytes) return CHLL_OK;
+  if (B->staging) cudaFree(B->staging);
+  B->staging = nullptr;
+  B->staging_bytes = 0;
+  BATCH_CUDA(cudaMalloc(&B->staging, bytes));
+  B->staging_bytes = bytes;
+  return CHLL_OK;
+}
+
+bool device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
+  if (!out) return fail(CHLL_EINVAL, "batch_create: null output pointer");
+  *out = nullptr;
+  if (!specs || n <= 0) return fail(CHLL_EINVAL, "batch_create: need at least one replica");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CHLL_ECUDA, "no CUDA device available; libchll_mod has no CPU path");
+  }
+  for (int r = 0; r < n; ++r) {
+    const chll_replica_spec& s = specs[r];
+    if (s.ni < 1 || s.nj < 1 || s.nk < 1)
+      return fail(CHLL_EINVAL, "batch_create: replica %d has dims %d %d %d", r, s.ni, s.nj, s.nk);
+    if (s.boundary != CHLL_OPEN && s.boundary != CHLL_PERIODIC)
+      return fail(CHLL_EINVAL, "batch_create: replica %d has boundary %d", r, s.boundary);
+    if (s.boundary == CHLL_PERIODIC && ((s.ni | s.nj | s.nk) & 1))
+      return fail(CHLL_EINVAL, "batch_create: replica %d is periodic with odd dims", r);
+    if (!(s.kT >= 0.0)) return fail(CHLL_EINVAL, "batch_create: replica %d has kT < 0", r);
+    const long long units = (long long)(chll::padded_ni(s.ni) / 4) * s.nj * s.nk;
+    if (units >= (1LL << 31))
+      return fail(CHLL_EINVAL, "batch_create: replica %d is too large", r);
+  }
+  chll::sweep_prepare();
+  chll_batch* B = new chll_batch();
+  B->n = n;
+  B->specs.assign(specs, specs + n);
+  cudaGetDevice(&B->sms);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, dev);
+  size_t slots = 0;
+  for (int r = 0; r < n; ++r) {
+    const chll_replica_spec& s = specs[r];
+    const size_t pc = (size_t)(chll::padded_ni(s.ni) / 2) * s.nj * s.nk;
+    B->offset.push_back(slots);
+    B->per_colour.push_back(pc);
+    slots += 2 * pc;
+    slots = (slots + 15) & ~(size_t)15;  // 256-byte aligned replica starts
+    B->total_sites += (long long)s.ni * s.nj * s.nk;
+  }
+  B->slots = slots;
+  auto bail = [&](cudaError_t e, const char* what) {
+    chll_batch_destroy(B);
+    return fail(e == cudaErrorMemoryAllocation ? CHLL_ENOMEM : CHLL_ECUDA, "batch_create: %s: %s",
+                what, cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&B->own_stream, cudaStreamNonBlocking))) return bail(e, "stream");
+  if ((e = cudaStreamCreateWithFlags(&B->capture_stream, cudaStreamNonBlocking)))
+    return bail(e, "stream");
+  B->stream = B->own_stream;
+  if ((e = cudaMalloc(&B->lat, slots * sizeof(float4)))) return bail(e, "lattices");
+  if ((e = cudaMemsetAsync(B->lat, 0, slots * sizeof(float4), B->stream))) return bail(e, "memset");
+  if ((e = cudaMalloc(&B->d_desc, sizeof(chll::ReplicaDesc) * n))) return bail(e, "descriptors");
+  if ((e = cudaMalloc(&B->d_state, sizeof(chll::ReplicaState) * n))) return bail(e, "states");
+  if ((e = cudaMalloc(&B->d_partials,
+                      sizeof(double) * chll::kObsMoments * B->sms * chll::kMaxCtasPerSm)))
+    return bail(e, "partials");
+  B->desc.resize(n);
+  std::vector<chll::ReplicaState> st(n);
+  for (int r = 0; r < n; ++r) {
+    const chll_replica_spec& s = specs[r];
+    chll::ReplicaDesc& D = B->desc[r];
+    std::memset(&D, 0, sizeof(D));
+    D.L.col[0] = B->lat + B->offset[r];
+    D.L.col[1] = B->lat + B->offset[r] + B->per_colour[r];
+    D.L.ni = s.ni;
+    D.L.nj = s.nj;
+    D.L.nk = s.nk;
+    D.L.hx = chll::padded_ni(s.ni) / 2;
+    D.L.periodic = s.boundary;
+    D.G = chll::make_geom(D.L);
+    D.cp.eps = (float)s.eps;
+    D.cp.K = (float)s.K;
+    D.cp.g = (float)s.g;
+    D.cp.inv_kT = (float)(1.0 / s.kT);
+    D.cd.eps = s.eps;
+    D.cd.K = s.K;
+    D.cd.g = s.g;
+    D.key0 = (uint32_t)s.seed;
+    D.key1 = (uint32_t)(s.seed >> 32);
+    D.replica = s.replica;
+    D.nsites = (long long)s.ni * s.nj * s.nk;
+    D.adapt_until = 10000;
+    std::memset(&st[r], 0, sizeof(chll::ReplicaState));
+    st[r].d = s.d;
+    st[r].step = 1;
+  }
+  if ((e = cudaMemcpyAsync(B->d_state, st.data(), sizeof(chll::ReplicaState) * n,
+                           cudaMemcpyHostToDevice, B->stream)))
+    return bail(e, "state upload");
+  if ((e = cudaStreamSynchronize(B->stream))) return bail(e, "sync");
+  *out = B;
+  return chll::record_ok();
+}
+
+void chll_batch_destroy(chll_batch* B) {
+  if (!B) return;
+  if (B->own_stream) cudaStreamSynchronize(B->own_stream);
+  if (B->stream && B->stream != B->own_stream) cudaStreamSynchronize(B->stream);
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  cudaFree(B->lat);
+  cudaFree(B->d_desc);
+  cudaFree(B->d_state);
+  cudaFree(B->d_cta_replica);
+  cudaFree(B->d_partials);
+  cudaFree(B->staging);
+  cudaFree(B->snap_lat);
+  cudaFree(B->snap_state);
+  if (B->own_stream) cudaStreamDestroy(B->own_stream);
+  if (B->capture_stream) cudaStreamDestroy(B->capture_stream);
+  delete B;
+}
+
+int chll_batch_set_stream(chll_batch* B, void* stream) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  B->stream = stream ? (cudaStream_t)stream : B->own_stream;
+  return chll::record_ok();
+}
+
+int chll_batch_sync(chll_batch* B) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  return chll::record_ok();
+}
+
+int chll_batch_init_random(chll_batch* B) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  for (int r = 0; r < B->n; ++r)
+    chll::launch_init_random(B->view(r), B->desc[r].key0, B->desc[r].key1, B->desc[r].replica,
+                             B->stream);
+  BATCH_CUDA(cudaGetLastError());
+  return chll::record_ok();
+}
+
+int chll_batch_upload_f4(chll_batch* B, int r, const float* xyzs) {
+  if (!B || !xyzs) return fail(CHLL_EINVAL, "batch_upload_f4: null argument");
+  if (r < 0 || r >= B->n) return fail(CHLL_EINVAL, "batch_upload_f4: replica %d out of range", r);
+  const size_t n = (size_t)B->desc[r].nsites;
+  const float4* src = (const float4*)xyzs;
+  if (!device_ptr(xyzs)) {
+    int rc = ensure_staging(B, n * sizeof(float4));
+    if (rc != CHLL_OK) return rc;
+    BATCH_CUDA(cudaMemcpyAsync(B->staging, xyzs, n * sizeof(float4), cudaMemcpyDefault,
+                               B->stream));
+    src = (const float4*)B->staging;
+  }
+  chll::launch_pack_f4(B->view(r), src, B->stream);
+  BATCH_CUDA(cudaGetLastError());
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  return chll::record_ok();
+}
+
+int chll_batch_download_f4(chll_batch* B, int r, float* xyzs) {
+  if (!B || !xyzs) return fail(CHLL_EINVAL, "batch_download_f4: null argument");
+  if (r < 0 || r >= B->n)
+    return fail(CHLL_EINVAL, "batch_download_f4: replica %d out of range", r);
+  const size_t n = (size_t)B->desc[r].nsites;
+  if (device_ptr(xyzs)) {
+    chll::launch_unpack_f4(B->view(r), (float4*)xyzs, B->stream);
+  } else {
+    int rc = ensure_staging(B, n * sizeof(float4));
+    if (rc != CHLL_OK) return rc;
+    chll::launch_unpack_f4(B->view(r), (float4*)B->staging, B->stream);
+    BATCH_CUDA(cudaMemcpyAsync(xyzs, B->staging, n * sizeof(float4), cudaMemcpyDefault,
+                               B->stream));
+  }
+  BATCH_CUDA(cudaGetLastError());
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  return chll::record_ok();
+}
+
+int chll_batch_run(chll_batch* B, int nsweeps, int measure_every, int measure_from) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  if (nsweeps < 0 || measure_every < 0)
+    return fail(CHLL_EINVAL, "batch_run: nsweeps and measure_every must be >= 0");
+  if (nsweeps == 0) return chll::record_ok();
+  const int rc = run_impl(B, nsweeps, measure_every, measure_from);
+  if (rc != CHLL_OK) return rc;
+  return chll::record_ok();
+}
+
+int chll_batch_moments(chll_batch* B, double* out) {
+  if (!B || !out) return fail(CHLL_EINVAL, "batch_moments: null argument");
+  std::vector<chll::ReplicaState> st(B->n);
+  BATCH_CUDA(cudaMemcpyAsync(st.data(), B->d_state, sizeof(chll::ReplicaState) * B->n,
+                             cudaMemcpyDeviceToHost, B->stream));
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  bool bad = false;
+  for (int r = 0; r < B->n; ++r) {
+    double* o = out + (size_t)r * chll::kMomLen;
+    for (int t = 0; t < 8; ++t) o[t] = st[r].mom[t];
+    o[8] = st[r].last[0];
+    o[9] = st[r].last[1];
+    o[10] = st[r].last[2];
+    o[11] = st[r].d;
+    o[12] = (double)st[r].step;
+    o[13] = st[r].paccept;
+    o[14] = st[r].faccept;
+    o[15] = (double)st[r].status;
+    bad = bad || st[r].status;
+  }
+  if (bad) return fail(CHLL_EDEVICE, "batch: a replica group barrier timed out");
+  return chll::record_ok();
+}
+
+int chll_batch_info(chll_batch* B, int64_t* total_sites, int32_t* nreplicas, int32_t* threads,
+                    int32_t* grid) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  const int rc = shape_launch(B);
+  if (rc != CHLL_OK) return rc;
+  if (total_sites) *total_sites = B->total_sites;
+  if (nreplicas) *nreplicas = B->n;
+  if (threads) *threads = B->threads;
+  if (grid) *grid = B->grid;
+  return chll::record_ok();
+}
+
+int chll_batch_set_tuning(chll_batch* B, int threads, int ctas_per_sm) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  if (threads != 128 && threads != 256 && threads != 512)
+    return fail(CHLL_EINVAL, "batch_set_tuning: threads must be 128, 256 or 512 (got %d)",
+                threads);
+  if (ctas_per_sm < 0 || ctas_per_sm > chll::kMaxCtasPerSm)
+    return fail(CHLL_EINVAL, "batch_set_tuning: ctas_per_sm must be 0..%d", chll::kMaxCtasPerSm);
+  if (threads * std::max(ctas_per_sm, 1) > 2048)
+    return fail(CHLL_EINVAL, "batch_set_tuning: more than 2048 threads per SM");
+  B->threads = threads;
+  B->ctas_per_sm = ctas_per_sm;
+  return chll::record_ok();
+}
+
+// Tries every (threads, CTAs per SM) shape that fits for `trial_sweeps`
+// sweeps from a snapshot of the current state, keeps the fastest, and
+// restores the snapshot.
+int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int* best_ctas,
+                        double* best_ms) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  if (trial_sweeps <= 0) return fail(CHLL_EINVAL, "batch_autotune: trial_sweeps must be > 0");
+  if (!B->snap_lat) BATCH_CUDA(cudaMalloc(&B->snap_lat, B->slots * sizeof(float4)));
+  if (!B->snap_state)
+    BATCH_CUDA(cudaMalloc(&B->snap_state, sizeof(chll::ReplicaState) * B->n));
+  BATCH_CUDA(cudaMemcpyAsync(B->snap_lat, B->lat, B->slots * sizeof(float4),
+                             cudaMemcpyDeviceToDevice, B->stream));
+  BATCH_CUDA(cudaMemcpyAsync(B->snap_state, B->d_state, sizeof(chll::ReplicaState) * B->n,
+                             cudaMemcpyDeviceToDevice, B->stream));
+  const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm;
+  cudaEvent_t e0, e1;
+  BATCH_CUDA(cudaEventCreate(&e0));
+  BATCH_CUDA(cudaEventCreate(&e1));
+  double best = 1e300;
+  int bt = keep_threads, bc = keep_ctas;
+  int rc = CHLL_OK;
+  for (int threads : {128, 256, 512}) {
+    const int occ = occupancy_of(threads);
+    for (int c = 1; c <= occ && rc == CHLL_OK; ++c) {
+      if (c * threads > 2048) break;
+      if (B->sms * c < B->n) continue;
+      B->threads = threads;
+      B->ctas_per_sm = c;
+      rc = shape_launch(B);
+      if (rc != CHLL_OK) break;
+      cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
+                      B->stream);
+      cudaMemcpyAsync(B->d_state, B->snap_state, sizeof(chll::ReplicaState) * B->n,
+                      cudaMemcpyDeviceToDevice, B->stream);
+      rc = launch_batch(B, B->stream, 1, 0, 0);  // warm-up
+      if (rc != CHLL_OK) break;
+      cudaEventRecord(e0, B->stream);
+      rc = launch_batch(B, B->stream, trial_sweeps, 0, 0);
+      if (rc != CHLL_OK) break;
+      cudaEventRecord(e1, B->stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        rc = fail(CHLL_ECUDA, "batch_autotune: %s", cudaGetErrorString(e));
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        bt = threads;
+        bc = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
+                  B->stream);
+  cudaMemcpyAsync(B->d_state, B->snap_state, sizeof(chll::ReplicaState) * B->n,
+                  cudaMemcpyDeviceToDevice, B->stream);
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  if (rc != CHLL_OK) {
+    B->threads = keep_threads;
+    B->ctas_per_sm = keep_ctas;
+    return rc;
+  }
+  B->threads = bt;
+  B->ctas_per_sm = bc;
+  if (best_threads) *best_threads = bt;
+  if (best_ctas) *best_ctas = bc;
+  if (best_ms) *best_ms = best;
+  return chll::record_ok();
+}
+
+}  // extern "C"

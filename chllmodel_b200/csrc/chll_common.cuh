@@ -79,6 +79,12 @@ struct LatticeView {
 
 __host__ __device__ __forceinline__ int padded_ni(int ni) { return (ni + 3) & ~3; }
 
+// Colour array by a runtime colour, as a select rather than an indexed load
+// (an indexed access would move the whole view to local memory).
+__host__ __device__ __forceinline__ float4* colour_array(const LatticeView& L, int c) {
+  return c ? L.col[1] : L.col[0];
+}
+
 // Division of x < 2^31 by a fixed divisor d >= 1 as one 32x32->64 multiply
 // and a shift: with s = ceil(log2 d), m = ceil(2^(31+s)/d) < 2^32 and
 // x*m = x*2^(31+s)/d + x*e/d (0 <= e < d), the error term is below

@@ -58,8 +58,10 @@ __device__ __forceinline__ void propose_director(float nx, float ny, float nz, f
   mz = z * r;
 }
 
-// One bond's contribution to E(m) - E(n) for a director trial n -> m.
-template <int AXIS, int SIGMA>
+// One bond's contribution to E(m) - E(n) for a director trial n -> m: the
+// nematic part into dn, and (s + s_b)*(dot_m*x_m - dot_o*x_o) into the
+// accumulator of its direction (+axis bonds carry sigma = -1, -axis +1).
+template <int AXIS>
 __device__ __forceinline__ void dir_bond(float nx, float ny, float nz, float mx, float my,
                                          float mz, float s, float4 b, float& dn, float& dc) {
   const float d_o = nx * b.x + ny * b.y + nz * b.z;
@@ -68,22 +70,21 @@ __device__ __forceinline__ void dir_bond(float nx, float ny, float nz, float mx,
   const float x_m = cross_axis<AXIS>(mx, my, mz, b);
   dn = fmaf(d_o, d_o, dn);
   dn = fmaf(-d_m, d_m, dn);
-  const float w = (float)SIGMA * 0.5f * (s + b.w);
-  dc = fmaf(w, fmaf(d_m, x_m, -d_o * x_o), dc);
+  dc = fmaf(s + b.w, fmaf(d_m, x_m, -d_o * x_o), dc);
 }
 
 // Energy difference of the director trial: eps*sum(dot_o^2 - dot_m^2) +
-// K*sum(sigma*sfac*(dot_m*x_m - dot_o*x_o)).
+// K*sum(sigma*sfac*(dot_m*x_m - dot_o*x_o)), sfac = (s + s_b)/2.
 __device__ __forceinline__ float director_dE(const float4& n, float mx, float my, float mz,
                                              const Nbrs& nb, const Coupling& cp) {
-  float dn = 0.f, dc = 0.f;
-  dir_bond<0, -1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[0], dn, dc);
-  dir_bond<0, +1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[1], dn, dc);
-  dir_bond<1, -1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[2], dn, dc);
-  dir_bond<1, +1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[3], dn, dc);
-  dir_bond<2, -1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[4], dn, dc);
-  dir_bond<2, +1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[5], dn, dc);
-  return fmaf(cp.eps, dn, cp.K * dc);
+  float dn = 0.f, dplus = 0.f, dminus = 0.f;
+  dir_bond<0>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[0], dn, dplus);
+  dir_bond<0>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[1], dn, dminus);
+  dir_bond<1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[2], dn, dplus);
+  dir_bond<1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[3], dn, dminus);
+  dir_bond<2>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[4], dn, dplus);
+  dir_bond<2>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[5], dn, dminus);
+  return fmaf(cp.eps, dn, 0.5f * cp.K * (dminus - dplus));
 }
 
 template <int AXIS, int SIGMA>

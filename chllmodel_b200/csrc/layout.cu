@@ -33,7 +33,7 @@ __global__ void pack_f64_kernel(LatticeView L, const double* __restrict__ nx,
        e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     site_of(L, e, i, j, k);
-    L.col[(i + j + k) & 1][slot(L, i, j, k)] =
+    colour_array(L, (i + j + k) & 1)[slot(L, i, j, k)] =
         make_float4((float)nx[e], (float)ny[e], (float)nz[e], (float)s[e]);
   }
 }
@@ -45,7 +45,7 @@ __global__ void unpack_f64_kernel(LatticeView L, double* __restrict__ nx, double
        e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     site_of(L, e, i, j, k);
-    const float4 v = L.col[(i + j + k) & 1][slot(L, i, j, k)];
+    const float4 v = colour_array(L, (i + j + k) & 1)[slot(L, i, j, k)];
     nx[e] = v.x;
     ny[e] = v.y;
     nz[e] = v.z;
@@ -59,7 +59,7 @@ __global__ void pack_f4_kernel(LatticeView L, const float4* __restrict__ src) {
        e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     site_of(L, e, i, j, k);
-    L.col[(i + j + k) & 1][slot(L, i, j, k)] = src[e];
+    colour_array(L, (i + j + k) & 1)[slot(L, i, j, k)] = src[e];
   }
 }
 
@@ -69,7 +69,7 @@ __global__ void unpack_f4_kernel(LatticeView L, float4* __restrict__ dst) {
        e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     site_of(L, e, i, j, k);
-    dst[e] = L.col[(i + j + k) & 1][slot(L, i, j, k)];
+    dst[e] = colour_array(L, (i + j + k) & 1)[slot(L, i, j, k)];
   }
 }
 
@@ -90,7 +90,7 @@ __global__ void init_random_kernel(LatticeView L, uint32_t key0, uint32_t key1,
     float sp, cp;
     sincospif(2.0f * u01(r.v[1]), &sp, &cp);
     const float s = (u01(r.v[2]) < 0.5f) ? -1.0f : 1.0f;
-    L.col[(i + j + k) & 1][slot(L, i, j, k)] = make_float4(st * cp, st * sp, ct, s);
+    colour_array(L, (i + j + k) & 1)[slot(L, i, j, k)] = make_float4(st * cp, st * sp, ct, s);
   }
 }
 

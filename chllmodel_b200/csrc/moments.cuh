@@ -1,0 +1,82 @@
+// FP64 moments of one lattice site, shared by the observables kernel
+// (observables.cu) and the batched kernel's measurements (batched.cu).
+//
+// Per site (FP64 arithmetic on the FP32 state), added into acc[0..8]:
+//   acc[0] total energy with the lattice's boundary, each bond once
+//          (+x, +y, +z) plus the field term;
+//   acc[1] the reference etot() sum (chll_mod.f90:414-456): x and y
+//          periodic, z open, and the +y dot product's x component read from
+//          the diagonal neighbour (ip1,jp1,k) exactly as chll_mod.f90:438;
+//   acc[2] s;  acc[3..8] nx*nx, ny*ny, nz*nz, nx*ny, nx*nz, ny*nz.
+#pragma once
+#include "chll_common.cuh"
+
+namespace chll {
+
+__device__ __forceinline__ float4 site_at(const LatticeView& L, int i, int j, int k) {
+  return colour_array(L, (i + j + k) & 1)[((size_t)k * L.nj + j) * L.hx + (i >> 1)];
+}
+
+// eps*(1 - dot^2) - K*dot*cross*sfac for a forward bond.
+__device__ __forceinline__ double fwd_bond(double eps, double K, double dot, double cross,
+                                           double si, double sj) {
+  return eps * (1.0 - dot * dot) - K * dot * cross * (0.5 * (si + sj));
+}
+
+// Storage slot e of the concatenated colour arrays (colour = e >= per_colour).
+__device__ __forceinline__ void site_moments(const LatticeView& L, const CouplingD& cp, size_t e,
+                                             size_t per_colour, double acc[kObsMoments]) {
+  const double eps = cp.eps, K = cp.K, g = cp.g;
+  const int c = e >= per_colour;
+  const size_t t = e - (c ? per_colour : 0);
+  const size_t r = t / (size_t)L.hx;
+  const int h = (int)(t - r * L.hx);
+  const int k = (int)(r / (size_t)L.nj);
+  const int j = (int)(r - (size_t)k * L.nj);
+  const int i = 2 * h + ((c + j + k) & 1);
+  if (i >= L.ni) return;
+  const float4 nf = colour_array(L, c)[t];
+  const double nx = nf.x, ny = nf.y, nz = nf.z, s = nf.w;
+  const int ip = (i + 1 == L.ni) ? 0 : i + 1;
+  const int jp = (j + 1 == L.nj) ? 0 : j + 1;
+  const int kp = (k + 1 == L.nk) ? 0 : k + 1;
+  const float4 X = site_at(L, ip, j, k);
+  const float4 Y = site_at(L, i, jp, k);
+  const float4 Z = site_at(L, i, j, kp);
+  const float4 T = site_at(L, ip, jp, k);  // diagonal read of chll_mod.f90:438
+
+  const double dx = nx * X.x + ny * X.y + nz * X.z;
+  const double cx = ny * X.z - nz * X.y;
+  const double bx = fwd_bond(eps, K, dx, cx, s, X.w);
+  const double dy = nx * Y.x + ny * Y.y + nz * Y.z;
+  const double cy = nz * Y.x - nx * Y.z;
+  const double by = fwd_bond(eps, K, dy, cy, s, Y.w);
+  const double dz = nx * Z.x + ny * Z.y + nz * Z.z;
+  const double cz = nx * Z.y - ny * Z.x;
+  const double bz = fwd_bond(eps, K, dz, cz, s, Z.w);
+
+  const bool has_xp = L.periodic || (i + 1 < L.ni);
+  const bool has_yp = L.periodic || (j + 1 < L.nj);
+  const bool has_zp = L.periodic || (k + 1 < L.nk);
+  acc[0] += (has_xp ? bx : 0.0) + (has_yp ? by : 0.0) + (has_zp ? bz : 0.0) - g * s;
+
+  const double dyt = nx * (double)T.x + ny * Y.y + nz * Y.z;
+  const double byt = fwd_bond(eps, K, dyt, cy, s, Y.w);
+  acc[1] += bx + byt + ((k + 1 < L.nk) ? bz : 0.0) - g * s;
+
+  acc[2] += s;
+  acc[3] += nx * nx;
+  acc[4] += ny * ny;
+  acc[5] += nz * nz;
+  acc[6] += nx * ny;
+  acc[7] += nx * nz;
+  acc[8] += ny * nz;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace chll

@@ -1,0 +1,156 @@
+// One work unit of a checkerboard half-sweep, shared by the plain pass
+// kernels (sweep.cu) and the batched persistent kernel (batched.cu), so that
+// a replica in a batch follows exactly the same chain as the same replica run
+// on its own.
+//
+// Unit g (row-major: g = q + Q*row, row = j + nj*k) is the two same-colour
+// sites of the 4-site x-block q of row (j,k): storage slots 2q and 2q+1 of
+// the colour-C array, lattice sites i0 = 4q + o and i1 = i0 + 2 with
+// o = (C+j+k)&1.  Both sites draw from one Philox call on the counter
+// {g, step, replica, pass}: director trials use words (0,1) and (2,3) as
+// (angle, acceptance), chirality trials words 0 and 2 as acceptance.
+#pragma once
+#include "chll_common.cuh"
+#include "chll_physics.cuh"
+
+namespace chll {
+
+struct SweepGeom {
+  uint32_t Q;      // units (4-site blocks) per row = hx/2
+  uint32_t units;  // Q * nj * nk
+  FastDiv by_Q;    // unit -> row
+  FastDiv by_nj;   // row -> plane
+};
+
+__host__ inline SweepGeom make_geom(const LatticeView& L) {
+  SweepGeom G;
+  G.Q = (uint32_t)(L.hx >> 1);
+  G.units = G.Q * (uint32_t)L.nj * (uint32_t)L.nk;
+  G.by_Q = FastDiv(G.Q);
+  G.by_nj = FastDiv((uint32_t)L.nj);
+  return G;
+}
+
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+
+// Updates unit g in place; returns the number of accepted trials (0..2).
+template <bool DIRECTOR, int C, bool PERIODIC>
+__device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const SweepGeom& G,
+                                                   uint32_t g, uint32_t step, float d,
+                                                   const Coupling& cp, uint32_t key0,
+                                                   uint32_t key1, uint32_t replica) {
+  constexpr uint32_t kPass = (DIRECTOR ? 0u : 2u) + (uint32_t)C;
+  const uint32_t hx = (uint32_t)L.hx;
+  const uint32_t nj = (uint32_t)L.nj, nk = (uint32_t)L.nk, ni = (uint32_t)L.ni;
+  const uint32_t plane = hx * nj;
+  const float4* __restrict__ oth = L.col[C ^ 1];
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+
+  const uint32_t row = G.by_Q.div(g);
+  const uint32_t q = g - row * G.Q;
+  const uint32_t k = G.by_nj.div(row);
+  const uint32_t j = row - k * nj;
+  const uint32_t o = (C + j + k) & 1u;
+  const uint32_t i0 = 4 * q + o;
+  const uint32_t i1 = i0 + 2;
+  const bool v0 = i0 < ni;
+  const bool v1 = i1 < ni;
+  const uint32_t rs = row * hx;  // slot of the row start
+  float4* cen = L.col[C] + rs + 2 * q;
+  float4 n0 = cen[0];
+  float4 n1 = cen[1];
+
+  // neighbour rows (slot offsets) and their presence
+  uint32_t sjm = rs - hx, sjp = rs + hx, skm = rs - plane, skp = rs + plane;
+  bool hjm = j > 0, hjp = j + 1 < nj, hkm = k > 0, hkp = k + 1 < nk;
+  // x neighbours of i0 and i1: xa = i0-1, xb = i0+1 = i1-1, xc = i1+1
+  uint32_t xa = i0 - 1, xb = i0 + 1, xc = i1 + 1;
+  bool hxa = i0 > 0, hxb = xb < ni, hxc = xc < ni;
+  if (PERIODIC) {
+    if (!hjm) sjm = rs + (nj - 1) * hx;
+    if (!hjp) sjp = rs - (nj - 1) * hx;
+    if (!hkm) skm = rs + (nk - 1) * plane;
+    if (!hkp) skp = rs - (nk - 1) * plane;
+    if (!hxa) xa = ni - 1;
+    if (!hxb) xb = 0;
+    if (!hxc) xc = 0;
+    hjm = hjp = hkm = hkp = hxa = hxb = hxc = true;
+  }
+  const float4* orow = oth + rs;
+  const float4 fa = hxa ? ld4(orow + (xa >> 1)) : zero;
+  const float4 fb = hxb ? ld4(orow + (xb >> 1)) : zero;
+  const float4 fc = hxc ? ld4(orow + (xc >> 1)) : zero;
+  const uint32_t h0 = 2 * q;
+  Nbrs nb0, nb1;
+  nb0.b[0] = fb;  // +x of i0
+  nb0.b[1] = fa;  // -x of i0
+  nb1.b[0] = fc;  // +x of i1
+  nb1.b[1] = fb;  // -x of i1
+  nb0.b[2] = hjp ? ld4(oth + sjp + h0) : zero;
+  nb1.b[2] = hjp ? ld4(oth + sjp + h0 + 1) : zero;
+  nb0.b[3] = hjm ? ld4(oth + sjm + h0) : zero;
+  nb1.b[3] = hjm ? ld4(oth + sjm + h0 + 1) : zero;
+  nb0.b[4] = hkp ? ld4(oth + skp + h0) : zero;
+  nb1.b[4] = hkp ? ld4(oth + skp + h0 + 1) : zero;
+  nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
+  nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
+
+  Ctr4 ctr = {{g, step, replica, kPass}};
+  const Ctr4 r = philox4x32_10(ctr, key0, key1);
+
+  unsigned int accepted = 0;
+  if (DIRECTOR) {
+    if (v0) {
+      float mx, my, mz;
+      propose_director(n0.x, n0.y, n0.z, d, u01(r.v[0]), mx, my, mz);
+      const float dE = director_dE(n0, mx, my, mz, nb0, cp);
+      if (metropolis(dE, u01(r.v[1]), cp.inv_kT)) {
+        n0.x = mx;
+        n0.y = my;
+        n0.z = mz;
+        ++accepted;
+      }
+    }
+    if (v1) {
+      float mx, my, mz;
+      propose_director(n1.x, n1.y, n1.z, d, u01(r.v[2]), mx, my, mz);
+      const float dE = director_dE(n1, mx, my, mz, nb1, cp);
+      if (metropolis(dE, u01(r.v[3]), cp.inv_kT)) {
+        n1.x = mx;
+        n1.y = my;
+        n1.z = mz;
+        ++accepted;
+      }
+    }
+  } else {
+    if (v0) {
+      const float dE = spin_dE(n0, nb0, cp);
+      if (metropolis(dE, u01(r.v[0]), cp.inv_kT)) {
+        n0.w = -n0.w;
+        ++accepted;
+      }
+    }
+    if (v1) {
+      const float dE = spin_dE(n1, nb1, cp);
+      if (metropolis(dE, u01(r.v[2]), cp.inv_kT)) {
+        n1.w = -n1.w;
+        ++accepted;
+      }
+    }
+  }
+  cen[0] = n0;
+  cen[1] = n1;
+  return accepted;
+}
+
+// The reference's step-size rule (chll_mod.f90:83-90): paccept is an FP32
+// fraction of N, the window is 0.4-0.6 in FP64 and the factor is the default
+// REAL literal 0.995.
+__host__ __device__ __forceinline__ double adapt_d(double d, float paccept) {
+  const double f = (double)0.995f;
+  if ((double)paccept < 0.4) return d * f;
+  if ((double)paccept > 0.6) return d / f;
+  return d;
+}
+
+}  // namespace chll

@@ -168,6 +168,68 @@ int chll_lattice_observe(chll_lattice* lat, const chll_coupling* c, double* row1
 int chll_lattice_energy_grad(chll_lattice* lat, const chll_coupling* c, float* grad, int project,
                              double* out4);
 
+/* ---- batched replicas (phase-diagram grids) ----------------------------- */
+
+/* One replica of a batch.  Its chain is the one chll_lattice_* would run for
+ * the same lattice: Philox key `seed`, counter word 2 `replica`, steps from 1,
+ * d adapted while step < 10000.  Replaces the reference's one-process-per-
+ * point drivers (scripts/phase_diagram.py:24-31, scripts/g_field0.5.py:24-31). */
+typedef struct chll_replica_spec {
+  int32_t ni, nj, nk, boundary;
+  double kT, K, g, eps, d;
+  uint64_t seed;
+  uint32_t replica;
+  uint32_t reserved;
+} chll_replica_spec;
+
+typedef struct chll_batch chll_batch;
+
+/* Columns of a chll_batch_moments row (FP64, 16 per replica). */
+#define CHLL_BATCH_NMEAS 0      /* number of measurements */
+#define CHLL_BATCH_SUM_E 1      /* sum of e = E/N */
+#define CHLL_BATCH_SUM_E2 2
+#define CHLL_BATCH_SUM_ETA 3    /* sum of eta = sum(s)/N */
+#define CHLL_BATCH_SUM_ETA2 4
+#define CHLL_BATCH_SUM_ABS_ETA 5
+#define CHLL_BATCH_SUM_S 6      /* sum of S = lambda_max(3/2 <n n> - I/2) */
+#define CHLL_BATCH_SUM_S2 7
+#define CHLL_BATCH_LAST_E 8
+#define CHLL_BATCH_LAST_ETA 9
+#define CHLL_BATCH_LAST_S 10
+#define CHLL_BATCH_D 11
+#define CHLL_BATCH_STEP 12      /* next step number */
+#define CHLL_BATCH_PACCEPT 13
+#define CHLL_BATCH_FACCEPT 14
+#define CHLL_BATCH_STATUS 15
+#define CHLL_BATCH_MOM_LEN 16
+
+/* Allocates n replicas of uneven sizes in one device allocation. */
+int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out);
+void chll_batch_destroy(chll_batch* b);
+int chll_batch_set_stream(chll_batch* b, void* stream);
+int chll_batch_sync(chll_batch* b);
+/* Every replica's random initial state from its own (seed, replica). */
+int chll_batch_init_random(chll_batch* b);
+/* Replica r's state as natural-order float4 records (host or device). */
+int chll_batch_upload_f4(chll_batch* b, int r, const float* xyzs);
+int chll_batch_download_f4(chll_batch* b, int r, float* xyzs);
+/* nsweeps steps of every replica in one persistent cooperative launch
+ * (captured once as a CUDA graph, replayed for equal arguments), measuring
+ * every measure_every sweeps from sweep measure_from of this call.
+ * Asynchronous on the batch's stream. */
+int chll_batch_run(chll_batch* b, int nsweeps, int measure_every, int measure_from);
+/* Waits, then copies n x CHLL_BATCH_MOM_LEN doubles to the host. */
+int chll_batch_moments(chll_batch* b, double* out);
+int chll_batch_info(chll_batch* b, int64_t* total_sites, int32_t* nreplicas, int32_t* threads,
+                    int32_t* grid);
+/* Launch shape: threads per CTA (128, 256, 512) and CTAs per SM (0: all that
+ * fit).  Each replica gets CTAs in proportion to its sites. */
+int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
+/* Times every launch shape for trial_sweeps sweeps from a snapshot of the
+ * current state, keeps the fastest and restores the state. */
+int chll_batch_autotune(chll_batch* b, int trial_sweeps, int* best_threads, int* best_ctas,
+                        double* best_ms);
+
 /* ---- energy adjoint without device allocation --------------------------- */
 
 /* Same results as chll_lattice_energy_grad, for callers that cannot let a
