@@ -173,9 +173,78 @@ __global__ void __launch_bounds__(kGradThreads)
   if (threadIdx.x == 0) *ticket = 0;
 }
 
+// One colour of a zero-temperature gradient quench: every site of colour C
+// moves against its tangent-projected energy gradient,
+//   n <- normalise(n - eta * (I - n n^T) dE/dn),
+// with the neighbours (the other colour) held fixed, so the two colours
+// alternate like the Metropolis half-sweeps.  Chiralities are not changed.
+template <int C>
+__global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L, Coupling cp,
+                                                                   float eta) {
+  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
+  float4* __restrict__ cen = L.col[C];
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < per_colour;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = t / (size_t)L.hx;
+    const int h = (int)(t - r * L.hx);
+    const int k = (int)(r / (size_t)L.nj);
+    const int j = (int)(r - (size_t)k * L.nj);
+    const int i = 2 * h + ((C + j + k) & 1);
+    if (i >= L.ni) continue;
+    float4 n = cen[t];
+    int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
+    bool hip = ip < L.ni, him = im >= 0, hjp = jp < L.nj, hjm = jm >= 0, hkp = kp < L.nk,
+         hkm = km >= 0;
+    if (L.periodic) {
+      if (!hip) ip = 0;
+      if (!him) im = L.ni - 1;
+      if (!hjp) jp = 0;
+      if (!hjm) jm = L.nj - 1;
+      if (!hkp) kp = 0;
+      if (!hkm) km = L.nk - 1;
+      hip = him = hjp = hjm = hkp = hkm = true;
+    }
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    bond_grad<0>(n, hip ? site(L, ip, j, k) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<0>(n, him ? site(L, im, j, k) : zero, +1.f, cp, gx, gy, gz);
+    bond_grad<1>(n, hjp ? site(L, i, jp, k) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<1>(n, hjm ? site(L, i, jm, k) : zero, +1.f, cp, gx, gy, gz);
+    bond_grad<2>(n, hkp ? site(L, i, j, kp) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<2>(n, hkm ? site(L, i, j, km) : zero, +1.f, cp, gx, gy, gz);
+    const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+    const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
+    const float x = n.x - eta * (gx - gn * n.x);
+    const float y = n.y - eta * (gy - gn * n.y);
+    const float z = n.z - eta * (gz - gn * n.z);
+    const float rn = rsqrtf(x * x + y * y + z * z);
+    n.x = x * rn;
+    n.y = y * rn;
+    n.z = z * rn;
+    cen[t] = n;
+  }
+}
+
 }  // namespace
 
 int energy_grad_max_blocks() { return kGradMaxBlocks; }
+
+void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, int colour,
+                        cudaStream_t stream) {
+  Coupling cp;
+  cp.eps = (float)cd.eps;
+  cp.K = (float)cd.K;
+  cp.g = (float)cd.g;
+  cp.inv_kT = 0.f;
+  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
+  size_t blocks = (per_colour + kGradThreads - 1) / kGradThreads;
+  if (blocks > (size_t)148 * 8) blocks = 148 * 8;
+  if (blocks == 0) blocks = 1;
+  if (colour == 0)
+    quench_pass_kernel<0><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, cp, eta);
+  else
+    quench_pass_kernel<1><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, cp, eta);
+}
 
 void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,
                         double* partials, unsigned int* ticket, double* out4,

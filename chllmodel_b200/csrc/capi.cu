@@ -803,6 +803,19 @@ int chll_lattice_observe(chll_lattice* L, const chll_coupling* c, double* row16)
   return ok();
 }
 
+int chll_lattice_quench(chll_lattice* L, const chll_coupling* c, double eta, int nsteps) {
+  if (!L || !c) return fail(CHLL_EINVAL, "quench: null argument");
+  if (nsteps < 0 || !(eta >= 0.0)) return fail(CHLL_EINVAL, "quench: need nsteps >= 0, eta >= 0");
+  const LatticeView v = L->view();
+  const chll::CouplingD cd = make_coupling_d(*c);
+  for (int s = 0; s < nsteps; ++s) {
+    chll::launch_quench_pass(v, cd, (float)eta, 0, L->stream);
+    chll::launch_quench_pass(v, cd, (float)eta, 1, L->stream);
+  }
+  CHLL_CUDA_TRY(cudaGetLastError());
+  return ok();
+}
+
 int chll_lattice_energy_grad(chll_lattice* L, const chll_coupling* c, float* grad, int project,
                              double* out4) {
   if (!L || !c) return fail(CHLL_EINVAL, "energy_grad: null argument");

@@ -33,5 +33,8 @@ void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_
                         double* partials, unsigned int* ticket, double* out4,
                         cudaStream_t stream);
 int energy_grad_max_blocks();
+// adjoint.cu: one colour of the zero-temperature gradient quench.
+void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, int colour,
+                        cudaStream_t stream);
 
 }  // namespace chll

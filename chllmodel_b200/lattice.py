@@ -149,6 +149,10 @@ class Lattice:
                                            row.ctypes.data_as(ct.c_void_p)))
         return row
 
+    def quench(self, cp: Coupling, eta: float, nsteps: int) -> None:
+        """nsteps of zero-temperature tangent gradient descent (asynchronous)."""
+        check(self._L.chll_lattice_quench(self._h, ct.byref(cp), float(eta), int(nsteps)))
+
     def energy_grad(self, cp: Coupling, project: bool = False, grad_ptr: int | None = None):
         """Returns (grad (N,4) host array or None if grad_ptr given, out4)."""
         out4 = np.zeros(4, np.float64)

@@ -128,7 +128,8 @@ typedef struct chll_coupling {
 int chll_lattice_create(int ni, int nj, int nk, int boundary, chll_lattice** out);
 void chll_lattice_destroy(chll_lattice* lat);
 /* Launch stream for all work on this lattice (a cudaStream_t; NULL restores
- * the lattice's own stream). */
+ * the lattice's own stream; cudaStreamLegacy (0x1) selects the legacy default
+ * stream). */
 int chll_lattice_set_stream(chll_lattice* lat, void* stream);
 int chll_lattice_sync(chll_lattice* lat);
 /* Random initial state: directors uniform on the sphere, s = +-1 with p=1/2. */
@@ -165,6 +166,10 @@ int chll_lattice_observe(chll_lattice* lat, const chll_coupling* c, double* row1
 /* Energy adjoint: grad (natural order float4, host or device, may be NULL)
  * receives dE/dn_i (w = 0), tangent-projected if project != 0; out4 (host)
  * receives {E, dE/deps, dE/dK, dE/dh} in FP64. */
+/* nsteps of zero-temperature gradient descent, n <- normalise(n - eta *
+ * tangent-projected dE/dn), colour 0 then colour 1 each step; chiralities
+ * fixed.  Asynchronous on the lattice's stream. */
+int chll_lattice_quench(chll_lattice* lat, const chll_coupling* c, double eta, int nsteps);
 int chll_lattice_energy_grad(chll_lattice* lat, const chll_coupling* c, float* grad, int project,
                              double* out4);
 
