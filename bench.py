@@ -350,7 +350,12 @@ def batched_vs_plain(args, rank, torch):
     b = Batch(specs)
     b.set_stream(stream.cuda_stream)
     b.init_random()
-    tune = b.autotune(trial_sweeps=20)
+    if args.batched_shape:
+        t, c = (int(x) for x in args.batched_shape.split("x"))
+        b.set_tuning(t, c)
+        tune = {"threads": t, "ctas_per_sm": c, "trial_ms": None}
+    else:
+        tune = b.autotune(trial_sweeps=20)
     b.run(nsw, measure_every=10)   # warm-up: graph capture and first launch
     b.sync()
     b.close()
@@ -370,8 +375,10 @@ def batched_vs_plain(args, rank, torch):
     info = b.info()
     b.close()
 
-    t_plain = 0.0
-    for sp in specs:
+    t_plain = float("nan")
+    for sp in ([] if args.no_plain_grid else specs):
+        if t_plain != t_plain:
+            t_plain = 0.0
         lat = Lattice(sp["ni"], sp["nj"], sp["nk"], boundary=sp["boundary"])
         lat.set_stream(stream.cuda_stream)
         lat.init_random(sp["seed"], sp["replica"])
@@ -415,6 +422,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-sweeps", type=int, default=2000)
+    ap.add_argument("--batched-shape", default="",
+                    help="THREADSxCTAS_PER_SM for the batched launch instead of autotuning")
+    ap.add_argument("--no-plain-grid", action="store_true",
+                    help="skip the sequential plain-kernel grid (profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--edge", type=int, default=L_EDGE,
                     help="lattice edge (480 is the benchmark; smaller edges for profiling)")
