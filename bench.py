@@ -32,6 +32,10 @@ L_EDGE = 480
 KT, KK, FIELD, EPS, D0, SEED = 0.3, 1.0, 0.0, 1.0, 0.1, 11
 NOUT = 100
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
+# DRAM read + write per site and launch of the pass kernels, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, mean of the four pass kernels)
+# on a 256^3 launch of the same kernels and scaled by sites to 480^3.
+TRAFFIC_BYTES_PER_SITE_PASS = 22.64
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
@@ -315,7 +319,9 @@ def gpu_arm(args):
                    "d0": D0, "nout": NOUT, "parallelism": f"replicas x{world}",
                    "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": achieved_gbs / peak, "traffic": None,
+                     "frac": achieved_gbs / peak,
+                     "traffic": TRAFFIC_BYTES_PER_SITE_PASS * n / 1e9,
+                     "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
                      "kernel": "sweep_pass_kernel (4 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
                      "ms_per_launch": pass_ms, "peak_kind": peak_kind},
