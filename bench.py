@@ -358,17 +358,18 @@ def batched_vs_plain(args, rank, torch):
     b.init_random()
     if args.batched_shape:
         t, c = (int(x) for x in args.batched_shape.split("x"))
-        b.set_tuning(t, c)
-        tune = {"threads": t, "ctas_per_sm": c, "trial_ms": None}
+        b.set_tuning(t, c, args.batched_wave_mb << 20)
+        tune = {"threads": t, "ctas_per_sm": c, "wave_bytes": args.batched_wave_mb << 20,
+                "trial_ms": None}
     else:
-        tune = b.autotune(trial_sweeps=20)
+        tune = b.autotune(trial_sweeps=100)
     b.run(nsw, measure_every=10)   # warm-up: graph capture and first launch
     b.sync()
     b.close()
     b = Batch(specs)
     b.set_stream(stream.cuda_stream)
     b.init_random()
-    b.set_tuning(tune["threads"], tune["ctas_per_sm"])
+    b.set_tuning(tune["threads"], tune["ctas_per_sm"], tune["wave_bytes"])
     b.sync()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -379,6 +380,7 @@ def batched_vs_plain(args, rank, torch):
     t_batched = e0.elapsed_time(e1) * 1e-3
     summ = b.summary()
     info = b.info()
+    info_tune = b.tuning()
     b.close()
 
     t_plain = float("nan")
@@ -412,7 +414,9 @@ def batched_vs_plain(args, rank, torch):
             "time_to_grid_s": t_batched, "sequential_plain_s": t_plain,
             "speedup_vs_sequential_plain": t_plain / t_batched,
             "site_updates_per_s": total * nsw / t_batched,
-            "tuning": {k: tune[k] for k in ("threads", "ctas_per_sm", "trial_ms")},
+            "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "trial_ms")},
+                           **{"waves": info_tune["waves"],
+                              "wave_MiB": info_tune["wave_bytes"] / 2 ** 20}),
             "grid_ctas": info["grid"],
             "mean_S_lowest_kT": float(np.mean([r["S"] for r in summ if r["kT"] < 0.2])),
             "mean_S_highest_kT": float(np.mean([r["S"] for r in summ if r["kT"] > 1.9]))}
@@ -430,6 +434,8 @@ def main():
     ap.add_argument("--batched-sweeps", type=int, default=2000)
     ap.add_argument("--batched-shape", default="",
                     help="THREADSxCTAS_PER_SM for the batched launch instead of autotuning")
+    ap.add_argument("--batched-wave-mb", type=int, default=0,
+                    help="wave size with --batched-shape (0: all replicas in one wave)")
     ap.add_argument("--no-plain-grid", action="store_true",
                     help="skip the sequential plain-kernel grid (profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -120,8 +120,17 @@ class Batch:
                                       ct.byref(g)))
         return {"total_sites": n.value, "replicas": r.value, "threads": t.value, "grid": g.value}
 
-    def set_tuning(self, threads, ctas_per_sm=0):
+    def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None):
         check(self._L.chll_batch_set_tuning(self._h, int(threads), int(ctas_per_sm)))
+        if wave_bytes is not None:
+            check(self._L.chll_batch_set_wave_bytes(self._h, int(wave_bytes)))
+
+    def tuning(self) -> dict:
+        t, c, w, n = ct.c_int32(), ct.c_int32(), ct.c_int64(), ct.c_int32()
+        check(self._L.chll_batch_get_tuning(self._h, ct.byref(t), ct.byref(c), ct.byref(w),
+                                            ct.byref(n)))
+        return {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": w.value,
+                "waves": n.value}
 
     def autotune(self, trial_sweeps=20, cache=None) -> dict:
         """Times every launch shape on this replica set and keeps the fastest.
@@ -131,13 +140,15 @@ class Batch:
             with open(cache) as f:
                 table = json.load(f)
             if key in table:
-                self.set_tuning(table[key]["threads"], table[key]["ctas_per_sm"])
-                return dict(table[key], cached=True)
+                e = table[key]
+                self.set_tuning(e["threads"], e["ctas_per_sm"], e.get("wave_bytes"))
+                return dict(e, cached=True)
         t, c, ms = ct.c_int(), ct.c_int(), ct.c_double()
         check(self._L.chll_batch_autotune(self._h, int(trial_sweeps), ct.byref(t), ct.byref(c),
                                           ct.byref(ms)))
-        res = {"threads": t.value, "ctas_per_sm": c.value, "trial_ms": ms.value,
-               "trial_sweeps": int(trial_sweeps)}
+        tun = self.tuning()
+        res = {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": tun["wave_bytes"],
+               "waves": tun["waves"], "trial_ms": ms.value, "trial_sweeps": int(trial_sweeps)}
         if cache:
             table = {}
             if os.path.exists(cache):

@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -160,12 +161,13 @@ __device__ __forceinline__ unsigned int group_pass(const ReplicaDesc& D, int ran
   return acc;
 }
 
+// All sweeps of one replica by its CTA group.  Returns false if the group's
+// status word was set (a barrier wait timed out).
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 768 / THREADS)
-    batch_kernel(const ReplicaDesc* __restrict__ descs, ReplicaState* __restrict__ states,
-                 const int* __restrict__ cta_replica, double* __restrict__ partials,
-                 int nsweeps, int measure_every, int measure_from, unsigned long long limit) {
-  const int rep = cta_replica[blockIdx.x];
+__device__ bool run_replica(const ReplicaDesc* __restrict__ descs,
+                            ReplicaState* __restrict__ states, int rep,
+                            double* __restrict__ partials, int nsweeps, int measure_every,
+                            int measure_from, unsigned long long limit) {
   const ReplicaDesc D = descs[rep];
   ReplicaState* st = states + rep;
   const int rank = (int)blockIdx.x - D.cta_first;
@@ -180,11 +182,11 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
     const int par = (int)(step & 1);
     // director trials: colour 0, colour 1 (chll_mod.f90:70,74)
     unsigned int acc = group_pass<true, 0, THREADS>(D, rank, step32, (float)d);
-    if (!group_barrier(st, nct, limit)) return;
+    if (!group_barrier(st, nct, limit)) return false;
     acc += group_pass<true, 1, THREADS>(D, rank, step32, (float)d);
     acc = cta_sum<THREADS>(acc);
     if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[par], (unsigned long long)acc);
-    if (!group_barrier(st, nct, limit)) return;
+    if (!group_barrier(st, nct, limit)) return false;
     // Every CTA of the group derives the same new d from the group's count
     // (chll_mod.f90:83-90); the director count of the other parity is reset
     // here for the next sweep (all CTAs finished reading it a sweep ago).
@@ -201,11 +203,11 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
     d = s_d;
     // chirality flips: colour 0, colour 1 (chll_mod.f90:78,81)
     acc = group_pass<false, 0, THREADS>(D, rank, step32, (float)d);
-    if (!group_barrier(st, nct, limit)) return;
+    if (!group_barrier(st, nct, limit)) return false;
     acc += group_pass<false, 1, THREADS>(D, rank, step32, (float)d);
     acc = cta_sum<THREADS>(acc);
     if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[2 + par], (unsigned long long)acc);
-    if (!group_barrier(st, nct, limit)) return;
+    if (!group_barrier(st, nct, limit)) return false;
     if (threadIdx.x == 0 && rank == 0) {
       const unsigned long long nf = *((volatile unsigned long long*)&st->cnt[2 + par]);
       st->faccept = (float)nf / n3;
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
         for (int w = 0; w < THREADS / 32; ++w) v += s_m[w][threadIdx.x];
         partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
       }
-      if (!group_barrier(st, nct, limit)) return;
+      if (!group_barrier(st, nct, limit)) return false;
       if (rank == 0 && threadIdx.x == 0) {
         double tot[kObsMoments];
         for (int t = 0; t < kObsMoments; ++t) tot[t] = 0.0;
@@ -266,6 +268,25 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
     st->d = d;
     st->step = step;
   }
+  return true;
+}
+
+// The persistent launch walks the waves in order: in wave w, CTA b works on
+// replica cta_map[w * gridDim.x + b] (-1: idle in this wave).  Waves hold
+// replicas whose state together fits in L2, so each wave's sweeps run from
+// L2; CTAs move to their next wave as soon as their replica is done.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 768 / THREADS)
+    batch_kernel(const ReplicaDesc* __restrict__ descs, ReplicaState* __restrict__ states,
+                 const int* __restrict__ cta_map, int nwaves, double* __restrict__ partials,
+                 int nsweeps, int measure_every, int measure_from, unsigned long long limit) {
+  for (int w = 0; w < nwaves; ++w) {
+    const int rep = cta_map[(size_t)w * gridDim.x + blockIdx.x];
+    if (rep < 0) continue;
+    if (!run_replica<THREADS>(descs, states, rep, partials, nsweeps, measure_every,
+                              measure_from, limit))
+      return;
+  }
 }
 
 }  // namespace
@@ -277,8 +298,8 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
 namespace chll {
 namespace {
 
-using BatchKernel = void (*)(const ReplicaDesc*, ReplicaState*, const int*, double*, int, int, int,
-                             unsigned long long);
+using BatchKernel = void (*)(const ReplicaDesc*, ReplicaState*, const int*, int, double*, int,
+                             int, int, unsigned long long);
 
 BatchKernel kernel_for(int threads) {
   switch (threads) {
@@ -332,8 +353,12 @@ struct chll_batch {
   int ctas_per_sm = 0;  // 0: as many as fit
   int grid = 0;         // CTAs of the current launch shape
   int shape_threads = -1, shape_ctas = -1;
+  long long wave_bytes = 0;  // state per wave (0: all replicas in one wave)
+  long long shape_wave_bytes = -1;
+  int nwaves = 1;
   cudaGraphExec_t graph = nullptr;
   int g_sweeps = -1, g_every = -1, g_from = -1, g_grid = -1, g_threads = -1;
+  long long g_waves = -1;
   unsigned long long limit = 1ull << 24;
   long long total_sites = 0;
 
@@ -350,57 +375,85 @@ int occupancy_of(int threads) {
   return n;
 }
 
-// CTAs per replica proportional to its units, at least one each, at most one
-// per `threads` units; fills desc[].cta_first/cta_count and the CTA map.
+// Splits the replicas into waves whose float4 state together stays within
+// wave_bytes (0: one wave), largest replicas first, and gives every replica of
+// a wave CTAs in proportion to its units (at least one, at most one per
+// `threads` units) out of the whole co-resident grid.  Fills
+// desc[].cta_first/cta_count and the per-wave CTA map (-1: idle).
 int shape_launch(chll_batch* B) {
-  if (B->shape_threads == B->threads && B->shape_ctas == B->ctas_per_sm && B->grid > 0)
+  if (B->shape_threads == B->threads && B->shape_ctas == B->ctas_per_sm &&
+      B->shape_wave_bytes == B->wave_bytes && B->grid > 0)
     return CHLL_OK;
   const int occ = occupancy_of(B->threads);
   if (occ <= 0) return fail(CHLL_ECUDA, "batch: kernel with %d threads cannot run", B->threads);
   const int per_sm = std::min(B->ctas_per_sm > 0 ? std::min(B->ctas_per_sm, occ) : occ,
                               chll::kMaxCtasPerSm);
   const int budget = B->sms * per_sm;
-  if (B->n > budget)
-    return fail(CHLL_ERANGE,
-                "batch: %d replicas need at least %d co-resident CTAs; this shape holds %d",
-                B->n, B->n, budget);
-  std::vector<double> units(B->n);
-  double tot = 0.0;
-  for (int r = 0; r < B->n; ++r) {
-    units[r] = (double)B->desc[r].G.units;
-    tot += units[r];
-  }
-  std::vector<int> cnt(B->n, 1);
-  std::vector<int> cap(B->n);
-  for (int r = 0; r < B->n; ++r)
-    cap[r] = std::max(1, (int)((B->desc[r].G.units + B->threads - 1) / B->threads));
-  int used = B->n;
-  // largest remainder on the share of the remaining CTAs
-  const int extra = budget - B->n;
-  std::vector<std::pair<double, int>> rem;
-  for (int r = 0; r < B->n; ++r) {
-    const double want = extra * units[r] / tot;
-    const int add = std::min((int)want, cap[r] - 1);
-    cnt[r] += add;
-    used += add;
-    rem.push_back({want - (int)want, r});
-  }
-  std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
-  for (auto& pr : rem) {
-    if (used >= budget) break;
-    if (cnt[pr.second] < cap[pr.second]) {
-      ++cnt[pr.second];
-      ++used;
+  // waves, largest first
+  std::vector<int> order(B->n);
+  for (int r = 0; r < B->n; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return B->desc[a].G.units > B->desc[b].G.units;
+  });
+  std::vector<std::vector<int>> waves;
+  std::vector<long long> wave_load;
+  for (int r : order) {
+    const long long bytes = (long long)(2 * B->per_colour[r] * sizeof(float4));
+    bool placed = false;
+    if (B->wave_bytes > 0) {
+      for (size_t w = 0; w < waves.size() && !placed; ++w) {
+        if (wave_load[w] + bytes <= B->wave_bytes && (int)waves[w].size() < budget) {
+          waves[w].push_back(r);
+          wave_load[w] += bytes;
+          placed = true;
+        }
+      }
+    } else if (!waves.empty() && (int)waves[0].size() < budget) {
+      waves[0].push_back(r);
+      wave_load[0] += bytes;
+      placed = true;
+    }
+    if (!placed) {
+      waves.push_back({r});
+      wave_load.push_back(bytes);
     }
   }
-  std::vector<int> map;
-  map.reserve(used);
-  for (int r = 0; r < B->n; ++r) {
-    B->desc[r].cta_first = (int)map.size();
-    B->desc[r].cta_count = cnt[r];
-    for (int c = 0; c < cnt[r]; ++c) map.push_back(r);
+  std::vector<int> map((size_t)waves.size() * budget, -1);
+  for (size_t w = 0; w < waves.size(); ++w) {
+    const std::vector<int>& reps = waves[w];
+    const int n = (int)reps.size();
+    double tot = 0.0;
+    for (int r : reps) tot += (double)B->desc[r].G.units;
+    std::vector<int> cnt(n, 1), cap(n);
+    for (int t = 0; t < n; ++t)
+      cap[t] = std::max(1, (int)((B->desc[reps[t]].G.units + B->threads - 1) / B->threads));
+    int used = n;
+    const int extra = budget - n;
+    std::vector<std::pair<double, int>> rem;
+    for (int t = 0; t < n; ++t) {
+      const double want = extra * (double)B->desc[reps[t]].G.units / tot;
+      const int add = std::min((int)want, cap[t] - 1);
+      cnt[t] += add;
+      used += add;
+      rem.push_back({want - (int)want, t});
+    }
+    std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    for (auto& pr : rem) {
+      if (used >= budget) break;
+      if (cnt[pr.second] < cap[pr.second]) {
+        ++cnt[pr.second];
+        ++used;
+      }
+    }
+    int next = 0;
+    for (int t = 0; t < n; ++t) {
+      B->desc[reps[t]].cta_first = next;
+      B->desc[reps[t]].cta_count = cnt[t];
+      for (int c = 0; c < cnt[t]; ++c) map[w * (size_t)budget + next++] = reps[t];
+    }
   }
-  B->grid = (int)map.size();
+  B->grid = budget;
+  B->nwaves = (int)waves.size();
   if (B->d_cta_replica) cudaFree(B->d_cta_replica);
   B->d_cta_replica = nullptr;
   BATCH_CUDA(cudaMalloc(&B->d_cta_replica, sizeof(int) * map.size()));
@@ -411,6 +464,7 @@ int shape_launch(chll_batch* B) {
   BATCH_CUDA(cudaStreamSynchronize(B->stream));
   B->shape_threads = B->threads;
   B->shape_ctas = B->ctas_per_sm;
+  B->shape_wave_bytes = B->wave_bytes;
   return CHLL_OK;
 }
 
@@ -427,7 +481,8 @@ int launch_batch(chll_batch* B, cudaStream_t s, int nsweeps, int every, int from
   cfg.numAttrs = 1;
   BATCH_CUDA(cudaLaunchKernelEx(&cfg, chll::kernel_for(B->threads),
                                 (const chll::ReplicaDesc*)B->d_desc, B->d_state,
-                                (const int*)B->d_cta_replica, B->d_partials, nsweeps, every, from,
+                                (const int*)B->d_cta_replica, B->nwaves, B->d_partials, nsweeps,
+                                every, from,
                                 B->limit));
   return CHLL_OK;
 }
@@ -436,7 +491,7 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
   int rc = shape_launch(B);
   if (rc != CHLL_OK) return rc;
   if (!(B->graph && B->g_sweeps == nsweeps && B->g_every == every && B->g_from == from &&
-        B->g_grid == B->grid && B->g_threads == B->threads)) {
+        B->g_grid == B->grid && B->g_threads == B->threads && B->g_waves == B->wave_bytes)) {
     if (B->graph) cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
     cudaGraph_t g = nullptr;
@@ -453,6 +508,7 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
     B->g_from = from;
     B->g_grid = B->grid;
     B->g_threads = B->threads;
+    B->g_waves = B->wave_bytes;
   }
   BATCH_CUDA(cudaGraphLaunch(B->graph, B->stream));
   return CHLL_OK;
@@ -699,6 +755,24 @@ int chll_batch_info(chll_batch* B, int64_t* total_sites, int32_t* nreplicas, int
   return chll::record_ok();
 }
 
+int chll_batch_set_wave_bytes(chll_batch* B, int64_t wave_bytes) {
+  if (!B || wave_bytes < 0) return fail(CHLL_EINVAL, "batch_set_wave_bytes: bad argument");
+  B->wave_bytes = wave_bytes;
+  return chll::record_ok();
+}
+
+int chll_batch_get_tuning(chll_batch* B, int32_t* threads, int32_t* ctas_per_sm,
+                          int64_t* wave_bytes, int32_t* nwaves) {
+  if (!B) return fail(CHLL_EINVAL, "null batch");
+  const int rc = shape_launch(B);
+  if (rc != CHLL_OK) return rc;
+  if (threads) *threads = B->threads;
+  if (ctas_per_sm) *ctas_per_sm = B->ctas_per_sm;
+  if (wave_bytes) *wave_bytes = B->wave_bytes;
+  if (nwaves) *nwaves = B->nwaves;
+  return chll::record_ok();
+}
+
 int chll_batch_set_tuning(chll_batch* B, int threads, int ctas_per_sm) {
   if (!B) return fail(CHLL_EINVAL, "null batch");
   if (threads != 128 && threads != 256 && threads != 512)
@@ -728,19 +802,25 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
   BATCH_CUDA(cudaMemcpyAsync(B->snap_state, B->d_state, sizeof(chll::ReplicaState) * B->n,
                              cudaMemcpyDeviceToDevice, B->stream));
   const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm;
+  const long long keep_waves = B->wave_bytes;
   cudaEvent_t e0, e1;
   BATCH_CUDA(cudaEventCreate(&e0));
   BATCH_CUDA(cudaEventCreate(&e1));
   double best = 1e300;
   int bt = keep_threads, bc = keep_ctas;
   int rc = CHLL_OK;
+  long long bw = B->wave_bytes;
+  // Candidates: one wave or 48 MiB waves; each block size at its two highest
+  // occupancies (lower occupancies were never faster on this kernel).
+  const long long kWaveOptions[] = {0ll, 48ll << 20};
+  for (long long wb : kWaveOptions)
   for (int threads : {128, 256, 512}) {
     const int occ = occupancy_of(threads);
-    for (int c = 1; c <= occ && rc == CHLL_OK; ++c) {
+    for (int c = std::max(1, occ - 1); c <= occ && rc == CHLL_OK; ++c) {
       if (c * threads > 2048) break;
-      if (B->sms * c < B->n) continue;
       B->threads = threads;
       B->ctas_per_sm = c;
+      B->wave_bytes = wb;
       rc = shape_launch(B);
       if (rc != CHLL_OK) break;
       cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
@@ -760,10 +840,14 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
       }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
+      if (std::getenv("CHLL_TUNE_VERBOSE"))
+        std::fprintf(stderr, "chll batch tune: threads %d ctas/SM %d wave %lld MiB waves %d: %.3f ms\n",
+                     threads, c, wb >> 20, B->nwaves, ms);
       if (ms < best) {
         best = ms;
         bt = threads;
         bc = c;
+        bw = wb;
       }
     }
   }
@@ -777,10 +861,12 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
   if (rc != CHLL_OK) {
     B->threads = keep_threads;
     B->ctas_per_sm = keep_ctas;
+    B->wave_bytes = keep_waves;
     return rc;
   }
   B->threads = bt;
   B->ctas_per_sm = bc;
+  B->wave_bytes = bw;
   if (best_threads) *best_threads = bt;
   if (best_ctas) *best_ctas = bc;
   if (best_ms) *best_ms = best;

@@ -230,8 +230,15 @@ int chll_batch_info(chll_batch* b, int64_t* total_sites, int32_t* nreplicas, int
 /* Launch shape: threads per CTA (128, 256, 512) and CTAs per SM (0: all that
  * fit).  Each replica gets CTAs in proportion to its sites. */
 int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
-/* Times every launch shape for trial_sweeps sweeps from a snapshot of the
- * current state, keeps the fastest and restores the state. */
+/* Replicas run in waves whose float4 state together stays within wave_bytes
+ * (0, the default: all replicas in one wave), largest first; each wave gets
+ * the whole co-resident grid, in the same launch. */
+int chll_batch_set_wave_bytes(chll_batch* b, int64_t wave_bytes);
+int chll_batch_get_tuning(chll_batch* b, int32_t* threads, int32_t* ctas_per_sm,
+                          int64_t* wave_bytes, int32_t* nwaves);
+/* Times every launch shape (threads, CTAs per SM, wave size) for trial_sweeps
+ * sweeps from a snapshot of the current state, keeps the fastest and restores
+ * the state. */
 int chll_batch_autotune(chll_batch* b, int trial_sweeps, int* best_threads, int* best_ctas,
                         double* best_ms);
 

@@ -25,15 +25,21 @@ def _specs():
     ]
 
 
-@pytest.mark.parametrize("threads", [128, 256, 512])
-def test_batch_replicas_equal_plain_runs(threads):
+@pytest.mark.parametrize("threads,wave_bytes", [(128, 0), (256, 1), (512, 48 << 20),
+                                                (128, 64 << 10)])
+def test_batch_replicas_equal_plain_runs(threads, wave_bytes):
+    """Any launch shape and wave split gives every replica its plain chain."""
     from chllmodel_b200.batched import Batch
     from chllmodel_b200.lattice import Lattice, coupling
 
     specs = _specs()
     nsw = 13
     with Batch(specs) as b:
-        b.set_tuning(threads, 0)
+        b.set_tuning(threads, 0, wave_bytes)
+        if wave_bytes == 1:
+            assert b.tuning()["waves"] == len(specs)  # every replica its own wave
+        if wave_bytes == 64 << 10:
+            assert b.tuning()["waves"] == 3  # 123 KB | 64 KB | 27 + 9 + 6 KB
         b.init_random()
         b.run(nsw, measure_every=4, measure_from=0)
         mom = b.moments()
