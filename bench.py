@@ -1,6 +1,7 @@
 """Benchmark of the plain checkerboard sweep: site updates/s and HBM roofline.
 
-Workload (one "step" = one full checkerboard sweep = 4 half-sweeps):
+Workload (one "step" = one full checkerboard sweep: director trials and
+chirality flips on both colours, run as the library's two fused passes):
   480^3 periodic lattice, eps=1, K=1, h=0, kT=0.3, directors uniform on the
   sphere and chiralities +-1 (Philox seed 11 + rank), d0 = 0.1 with the
   reference's adaptation, FP64 observables every 100 sweeps.  The float4
@@ -32,10 +33,10 @@ L_EDGE = 480
 KT, KK, FIELD, EPS, D0, SEED = 0.3, 1.0, 0.0, 1.0, 0.1, 11
 NOUT = 100
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
-# DRAM read + write per site and launch of the pass kernels, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum, mean of the four pass kernels)
-# on a 256^3 launch of the same kernels and scaled by sites to 480^3.
-TRAFFIC_BYTES_PER_SITE_PASS = 22.64
+# DRAM read + write per site and launch of the fused pass kernels, measured
+# with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
+# B) on a 256^3 launch and scaled by sites to 480^3; None until measured.
+TRAFFIC_BYTES_PER_SITE_PASS = None
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
@@ -204,7 +205,7 @@ def gpu_arm(args):
         torch.cuda.synchronize()
 
     from chllmodel_b200 import chll
-    from chllmodel_b200.lattice import Lattice, coupling
+    from chllmodel_b200.lattice import FUSED_A, FUSED_A0, FUSED_B, FUSED_F, Lattice, coupling
 
     edge = args.edge
     n = edge ** 3
@@ -214,50 +215,79 @@ def gpu_arm(args):
     lat.set_stream(stream.cuda_stream)
     lat.init_random(SEED + rank)
     lat.set_control(D0, step=1)
-    nmeas = args.steps // NOUT + 2
+    nmeas = (args.steps + args.warmup) // NOUT + 2
     lat.reserve_rows(nmeas)
 
-    # warm-up (captures the 1-sweep graph)
+    # One step = one sweep in the library's fused form (chll_lattice_sweep's
+    # graph holds the same launches): pass A (A0 after a closed step) and
+    # pass B per sweep, the closing colour-0 flip pass F before each FP64
+    # measurement and after the last sweep.  Every A/B launch is bracketed by
+    # CUDA events on its stream: their mean is the roofline's launch time.
+    class Runner:
+        """Issues sweeps as fused passes and FP64 measurements into row slots."""
+
+        def __init__(self):
+            self.slot = 0  # last row slot written
+
+        def sweeps(self, count, first_step, events=None):
+            pending, nl = False, 0
+            for i in range(count):
+                e = None
+                if events is not None:
+                    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                    e[0].record(stream)
+                lat.half_sweep(cp, FUSED_A if pending else FUSED_A0, seed=SEED, replica=rank)
+                if e:
+                    e[1].record(stream)
+                lat.half_sweep(cp, FUSED_B, seed=SEED, replica=rank)
+                if e:
+                    e[2].record(stream)
+                    events.append(e)
+                nl += 2
+                pending = True
+                meas = (first_step + i) % NOUT == 0
+                if meas or i == count - 1:
+                    lat.half_sweep(cp, FUSED_F, seed=SEED, replica=rank)
+                    nl += 1
+                    pending = False
+                if meas:
+                    self.slot += 1
+                    lat.measure(cp, self.slot)
+                    nl += 1
+            return nl
+
+    runner = Runner()
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            lat.sweep(cp, 1, seed=SEED, replica=rank)
-        lat.measure(cp, 0)
+        runner.sweeps(args.warmup, 1)
     lat.sync()
     step0 = args.warmup + 1
 
     ev_start = torch.cuda.Event(enable_timing=True)
     ev_end = torch.cuda.Event(enable_timing=True)
-    sw_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    sw_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    launches = 0
+    pass_events = []
     barrier()
     with ClockSampler(local) as clocks:
         ev_start.record(stream)
-        slot = 0
-        for i in range(args.steps):
-            sw_s[i].record(stream)
-            lat.sweep(cp, 1, seed=SEED, replica=rank)
-            sw_e[i].record(stream)
-            launches += 4
-            if (step0 + i) % NOUT == 0:
-                slot += 1
-                lat.measure(cp, slot)
-                launches += 1
+        slot_first = runner.slot + 1
+        launches = runner.sweeps(args.steps, step0, pass_events)
         ev_end.record(stream)
         ev_end.synchronize()
     barrier()
+    slot = runner.slot
     ms = ev_start.elapsed_time(ev_end)
-    sweep_ms = sum(a.elapsed_time(b) for a, b in zip(sw_s, sw_e))
-    t = torch.tensor([ms, sweep_ms], device="cuda", dtype=torch.float64)
+    a_ms = sum(e[0].elapsed_time(e[1]) for e in pass_events)
+    b_ms = sum(e[1].elapsed_time(e[2]) for e in pass_events)
+    t = torch.tensor([ms, a_ms, b_ms], device="cuda", dtype=torch.float64)
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, sweep_ms = float(t[0]), float(t[1])
+    ms, a_ms, b_ms = float(t[0]), float(t[1]), float(t[2])
     value = world * n * args.steps / (ms * 1e-3)
-    pass_ms = sweep_ms / (4 * args.steps)
+    pass_ms = (a_ms + b_ms) / (2 * args.steps)
     achieved_gbs = BYTES_PER_SITE_PASS * n / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = _peaks()
     ctl = lat.control()
-    rows = lat.read_rows(1, slot) if slot else np.zeros((0, 16))
+    rows = lat.read_rows(slot_first, slot - slot_first + 1) if slot >= slot_first \
+        else np.zeros((0, 16))
     lat.close()
     del lat
 
@@ -320,11 +350,15 @@ def gpu_arm(args):
                    "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak,
-                     "traffic": TRAFFIC_BYTES_PER_SITE_PASS * n / 1e9,
+                     "traffic": (TRAFFIC_BYTES_PER_SITE_PASS * n / 1e9
+                                 if TRAFFIC_BYTES_PER_SITE_PASS else None),
                      "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
-                     "kernel": "sweep_pass_kernel (4 launches per step)",
+                     "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
-                     "ms_per_launch": pass_ms, "peak_kind": peak_kind},
+                     "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
+                     "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,
+                     "four_half_sweep_equiv_gbs": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)
+                     * args.steps / 1e9},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
@@ -362,7 +396,7 @@ def batched_vs_plain(args, rank, torch):
         tune = {"threads": t, "ctas_per_sm": c, "wave_bytes": args.batched_wave_mb << 20,
                 "trial_ms": None}
     else:
-        tune = b.autotune(trial_sweeps=100)
+        tune = b.autotune(trial_sweeps=200)
     b.run(nsw, measure_every=10)   # warm-up: graph capture and first launch
     b.sync()
     b.close()

@@ -31,6 +31,7 @@ EXPORTS = (
     "chll_lattice_sweep", "chll_lattice_pass", "chll_lattice_observe",
     "chll_lattice_energy_grad", "chll_lattice_reserve_rows", "chll_lattice_measure",
     "chll_lattice_read_rows", "chll_energy_grad_noalloc", "chll_lattice_quench",
+    "chll_lattice_set_kernel",
     "chll_batch_create", "chll_batch_destroy", "chll_batch_set_stream", "chll_batch_sync",
     "chll_batch_init_random", "chll_batch_upload_f4", "chll_batch_download_f4", "chll_batch_run",
     "chll_batch_moments", "chll_batch_info", "chll_batch_set_tuning", "chll_batch_autotune",
@@ -138,6 +139,8 @@ def _declare(L: ct.CDLL) -> None:
     L.chll_lattice_pass.argtypes = [vp, P(Coupling), u64, u32, i32]
     L.chll_lattice_observe.argtypes = [vp, P(Coupling), vp]
     L.chll_lattice_energy_grad.argtypes = [vp, P(Coupling), vp, i32, vp]
+    L.chll_lattice_set_kernel.argtypes = [vp, i32]
+    L.chll_lattice_set_kernel.restype = i32
     L.chll_lattice_quench.argtypes = [vp, P(Coupling), dbl, i32]
     L.chll_lattice_quench.restype = i32
     L.chll_lattice_reserve_rows.argtypes = [vp, i32]

@@ -15,7 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchll_mod.so")
 SOURCES = ["sweep.cu", "batched.cu", "layout.cu", "observables.cu", "adjoint.cu", "capi.cu",
            "noalloc.cu"]
-HEADERS = ["chll_common.cuh", "chll_physics.cuh", "sweep.cuh", "sweep_unit.cuh", "moments.cuh"]
+HEADERS = ["chll_common.cuh", "chll_physics.cuh", "sweep.cuh", "sweep_unit.cuh", "moments.cuh",
+           "staged.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -62,7 +62,7 @@ struct ReplicaDesc {
 struct ReplicaState {
   double d;
   long long step;
-  unsigned long long cnt[4];  // director counts by sweep parity [0,1], flips [2,3]
+  unsigned long long cnt[4];  // director counts by step parity [0,1], flips [2,3]
   unsigned int bar_count;
   unsigned int bar_gen;
   unsigned int status;
@@ -120,7 +120,7 @@ __device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limi
             atomicOr(&st->status, 1u);
             break;
           }
-          __nanosleep(100);
+          if (it > 64) __nanosleep(32);
         }
       }
       __threadfence();
@@ -131,34 +131,111 @@ __device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limi
   return s_ok != 0;
 }
 
+// CTA sums of three counts, valid in thread 0.
 template <int THREADS>
-__device__ __forceinline__ unsigned int cta_sum(unsigned int v) {
-  __shared__ unsigned int s_w[THREADS / 32];
-  v = __reduce_add_sync(0xffffffffu, v);
-  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+__device__ __forceinline__ void cta_sum3(unsigned int& a, unsigned int& b, unsigned int& c) {
+  __shared__ unsigned int s_w[3][THREADS / 32];
+  a = __reduce_add_sync(0xffffffffu, a);
+  b = __reduce_add_sync(0xffffffffu, b);
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) {
+    s_w[0][threadIdx.x >> 5] = a;
+    s_w[1][threadIdx.x >> 5] = b;
+    s_w[2][threadIdx.x >> 5] = c;
+  }
   __syncthreads();
-  unsigned int t = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < THREADS / 32; ++w) t += s_w[w];
+  if (threadIdx.x == 0) {
+    a = b = c = 0;
+    for (int w = 0; w < THREADS / 32; ++w) {
+      a += s_w[0][w];
+      b += s_w[1][w];
+      c += s_w[2][w];
+    }
+  }
   __syncthreads();
-  return t;  // valid in thread 0
 }
 
-template <bool DIRECTOR, int C, int THREADS>
-__device__ __forceinline__ unsigned int group_pass(const ReplicaDesc& D, int rank, uint32_t step,
-                                                   float d) {
-  unsigned int acc = 0;
-  const uint32_t stride = (uint32_t)D.cta_count * THREADS;
-  if (D.L.periodic) {
-    for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units; g += stride)
-      acc += sweep_unit<DIRECTOR, C, true>(D.L, D.G, g, step, d, D.cp, D.key0, D.key1,
-                                           D.replica);
-  } else {
-    for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units; g += stride)
-      acc += sweep_unit<DIRECTOR, C, false>(D.L, D.G, g, step, d, D.cp, D.key0, D.key1,
-                                            D.replica);
+// One fused pass (sweep.cuh FusedPhase) of a replica by its CTA group: the
+// group's CTAs walk the replica's units grid-stride with the plain kernels'
+// unit_step, so the chain is the one the replica follows alone.
+template <int PHASE, bool PERIODIC, int THREADS>
+__device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
+                                           uint32_t step, float d, unsigned int& nacc,
+                                           unsigned int& nflip) {
+  constexpr int C = PHASE == kFusedB ? 1 : 0;
+  constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
+  constexpr bool DIR = PHASE != kFusedF;
+  constexpr bool FLIP_AFTER = PHASE == kFusedB;
+  for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units;
+       g += (uint32_t)nct * THREADS)
+    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(D.L, D.G, g, step, d, D.cp, D.key0,
+                                                         D.key1, D.replica, nacc, nflip);
+}
+
+template <int PHASE, int THREADS>
+__device__ __forceinline__ void group_pass(const ReplicaDesc& D, int rank, int nct,
+                                           uint32_t step, float d, unsigned int& nacc,
+                                           unsigned int& nflip) {
+  if (D.L.periodic)
+    group_loop<PHASE, true, THREADS>(D, rank, nct, step, d, nacc, nflip);
+  else
+    group_loop<PHASE, false, THREADS>(D, rank, nct, step, d, nacc, nflip);
+}
+
+// FP64 moments of one replica's current state (moments.cuh), summed by its
+// first CTA in a fixed order and accumulated into its state block.  Kept out
+// of line: it runs once per measurement and its FP64 registers would
+// otherwise crowd the sweep loop.
+template <int THREADS>
+__device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState* st, int rank,
+                                             int nct, double* __restrict__ partials,
+                                             unsigned long long limit) {
+  double m[kObsMoments];
+#pragma unroll
+  for (int t = 0; t < kObsMoments; ++t) m[t] = 0.0;
+  const size_t per_colour = (size_t)D.L.hx * D.L.nj * D.L.nk;
+  const size_t total = 2 * per_colour;
+  for (size_t e = (size_t)rank * THREADS + threadIdx.x; e < total;
+       e += (size_t)nct * THREADS)
+    site_moments(D.L, D.cd, e, per_colour, m);
+  __shared__ double s_m[THREADS / 32][kObsMoments];
+#pragma unroll
+  for (int t = 0; t < kObsMoments; ++t) {
+    const double v = warp_sum_d(m[t]);
+    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5][t] = v;
   }
-  return acc;
+  __syncthreads();
+  if (threadIdx.x < kObsMoments) {
+    double v = 0.0;
+    for (int w = 0; w < THREADS / 32; ++w) v += s_m[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
+  }
+  if (!group_barrier(st, nct, limit)) return false;
+  if (rank == 0 && threadIdx.x == 0) {
+    double tot[kObsMoments];
+    for (int t = 0; t < kObsMoments; ++t) tot[t] = 0.0;
+    for (int c = 0; c < nct; ++c)
+      for (int t = 0; t < kObsMoments; ++t)
+        tot[t] += *((volatile double*)&partials[(size_t)(D.cta_first + c) * kObsMoments + t]);
+    const double n = (double)D.nsites;
+    const double e = tot[0] / n, eta = tot[2] / n;
+    const double qxx = 1.5 * tot[3] / n - 0.5, qyy = 1.5 * tot[4] / n - 0.5,
+                 qzz = 1.5 * tot[5] / n - 0.5;
+    const double qxy = 1.5 * tot[6] / n, qxz = 1.5 * tot[7] / n, qyz = 1.5 * tot[8] / n;
+    const double S = sym3_max_eig(qxx, qyy, qzz, qxy, qxz, qyz);
+    st->mom[0] += 1.0;
+    st->mom[1] += e;
+    st->mom[2] += e * e;
+    st->mom[3] += eta;
+    st->mom[4] += eta * eta;
+    st->mom[5] += fabs(eta);
+    st->mom[6] += S;
+    st->mom[7] += S * S;
+    st->last[0] = e;
+    st->last[1] = eta;
+    st->last[2] = S;
+  }
+  return true;
 }
 
 // All sweeps of one replica by its CTA group.  Returns false if the group's
@@ -168,7 +245,7 @@ __device__ bool run_replica(const ReplicaDesc* __restrict__ descs,
                             ReplicaState* __restrict__ states, int rep,
                             double* __restrict__ partials, int nsweeps, int measure_every,
                             int measure_from, unsigned long long limit) {
-  const ReplicaDesc D = descs[rep];
+  const ReplicaDesc& D = descs[rep];
   ReplicaState* st = states + rep;
   const int rank = (int)blockIdx.x - D.cta_first;
   const int nct = D.cta_count;
@@ -177,92 +254,66 @@ __device__ bool run_replica(const ReplicaDesc* __restrict__ descs,
   long long step = st->step;
   __shared__ double s_d;
 
+  // The fused two-pass sweep of the plain kernels (sweep.cu): pass A = the
+  // previous sweep's colour-0 flips (when pending) + colour-0 director
+  // trials, pass B = colour-1 director trials + colour-1 flips, and a
+  // colour-0 flip pass F closes the sweep before a measurement and after the
+  // last sweep.  Counts: director accepts of step t in cnt[t&1], flips of
+  // step t in cnt[2 + (t&1)].
+  bool pending = false;
   for (int s = 0; s < nsweeps; ++s, ++step) {
     const uint32_t step32 = (uint32_t)step;
     const int par = (int)(step & 1);
-    // director trials: colour 0, colour 1 (chll_mod.f90:70,74)
-    unsigned int acc = group_pass<true, 0, THREADS>(D, rank, step32, (float)d);
+    const int done = s + 1;
+    const bool measure =
+        measure_every > 0 && done >= measure_from && done % measure_every == 0;
+    const bool flush = measure || done == nsweeps;
+    unsigned int na = 0, nf_prev = 0, nf = 0;
+    if (pending)
+      group_pass<kFusedA, THREADS>(D, rank, nct, step32, (float)d, na, nf_prev);
+    else
+      group_pass<kFusedA0, THREADS>(D, rank, nct, step32, (float)d, na, nf_prev);
     if (!group_barrier(st, nct, limit)) return false;
-    acc += group_pass<true, 1, THREADS>(D, rank, step32, (float)d);
-    acc = cta_sum<THREADS>(acc);
-    if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[par], (unsigned long long)acc);
+    group_pass<kFusedB, THREADS>(D, rank, nct, step32, (float)d, na, nf);
+    if (flush) {
+      if (!group_barrier(st, nct, limit)) return false;
+      group_pass<kFusedF, THREADS>(D, rank, nct, step32 + 1u, (float)d, na, nf);
+    }
+    cta_sum3<THREADS>(na, nf_prev, nf);
+    if (threadIdx.x == 0) {
+      if (na) atomicAdd(&st->cnt[par], (unsigned long long)na);
+      if (nf_prev) atomicAdd(&st->cnt[2 + (par ^ 1)], (unsigned long long)nf_prev);
+      if (nf) atomicAdd(&st->cnt[2 + par], (unsigned long long)nf);
+    }
     if (!group_barrier(st, nct, limit)) return false;
     // Every CTA of the group derives the same new d from the group's count
-    // (chll_mod.f90:83-90); the director count of the other parity is reset
-    // here for the next sweep (all CTAs finished reading it a sweep ago).
+    // (chll_mod.f90:83-90).  The counters read here are reset by the group's
+    // first CTA for their next use, which no CTA reaches before it passes the
+    // next barrier.
     if (threadIdx.x == 0) {
-      const unsigned long long na = *((volatile unsigned long long*)&st->cnt[par]);
-      const float pa = (float)na / n3;
+      const unsigned long long na_all = *((volatile unsigned long long*)&st->cnt[par]);
+      const float pa = (float)na_all / n3;
       s_d = (step < D.adapt_until) ? adapt_d(d, pa) : d;
       if (rank == 0) {
         st->cnt[par ^ 1] = 0;
         st->paccept = pa;
+        if (pending) {  // flips of step-1 are complete (chll_mod.f90:93)
+          st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + (par ^ 1)]) / n3;
+          st->cnt[2 + (par ^ 1)] = 0;
+        }
+        if (flush) {
+          st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + par]) / n3;
+          st->cnt[2 + par] = 0;
+        }
       }
     }
     __syncthreads();
     d = s_d;
-    // chirality flips: colour 0, colour 1 (chll_mod.f90:78,81)
-    acc = group_pass<false, 0, THREADS>(D, rank, step32, (float)d);
-    if (!group_barrier(st, nct, limit)) return false;
-    acc += group_pass<false, 1, THREADS>(D, rank, step32, (float)d);
-    acc = cta_sum<THREADS>(acc);
-    if (threadIdx.x == 0 && acc) atomicAdd(&st->cnt[2 + par], (unsigned long long)acc);
-    if (!group_barrier(st, nct, limit)) return false;
-    if (threadIdx.x == 0 && rank == 0) {
-      const unsigned long long nf = *((volatile unsigned long long*)&st->cnt[2 + par]);
-      st->faccept = (float)nf / n3;
-      st->cnt[2 + (par ^ 1)] = 0;
-    }
+    pending = !flush;
 
-    // FP64 measurement
-    const int done = s + 1;
-    if (measure_every > 0 && done >= measure_from && done % measure_every == 0) {
-      double m[kObsMoments];
-#pragma unroll
-      for (int t = 0; t < kObsMoments; ++t) m[t] = 0.0;
-      const size_t per_colour = (size_t)D.L.hx * D.L.nj * D.L.nk;
-      const size_t total = 2 * per_colour;
-      for (size_t e = (size_t)rank * THREADS + threadIdx.x; e < total;
-           e += (size_t)nct * THREADS)
-        site_moments(D.L, D.cd, e, per_colour, m);
-      __shared__ double s_m[THREADS / 32][kObsMoments];
-#pragma unroll
-      for (int t = 0; t < kObsMoments; ++t) {
-        const double v = warp_sum_d(m[t]);
-        if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5][t] = v;
-      }
-      __syncthreads();
-      if (threadIdx.x < kObsMoments) {
-        double v = 0.0;
-        for (int w = 0; w < THREADS / 32; ++w) v += s_m[w][threadIdx.x];
-        partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
-      }
-      if (!group_barrier(st, nct, limit)) return false;
-      if (rank == 0 && threadIdx.x == 0) {
-        double tot[kObsMoments];
-        for (int t = 0; t < kObsMoments; ++t) tot[t] = 0.0;
-        for (int c = 0; c < nct; ++c)
-          for (int t = 0; t < kObsMoments; ++t)
-            tot[t] += *((volatile double*)&partials[(size_t)(D.cta_first + c) * kObsMoments + t]);
-        const double n = (double)D.nsites;
-        const double e = tot[0] / n, eta = tot[2] / n;
-        const double qxx = 1.5 * tot[3] / n - 0.5, qyy = 1.5 * tot[4] / n - 0.5,
-                     qzz = 1.5 * tot[5] / n - 0.5;
-        const double qxy = 1.5 * tot[6] / n, qxz = 1.5 * tot[7] / n, qyz = 1.5 * tot[8] / n;
-        const double S = sym3_max_eig(qxx, qyy, qzz, qxy, qxz, qyz);
-        st->mom[0] += 1.0;
-        st->mom[1] += e;
-        st->mom[2] += e * e;
-        st->mom[3] += eta;
-        st->mom[4] += eta * eta;
-        st->mom[5] += fabs(eta);
-        st->mom[6] += S;
-        st->mom[7] += S * S;
-        st->last[0] = e;
-        st->last[1] = eta;
-        st->last[2] = S;
-      }
-    }
+    // FP64 measurement of the completed sweep
+    if (measure)
+      if (!measure_replica<THREADS>(D, st, rank, nct, partials, limit)) return false;
   }
   if (rank == 0 && threadIdx.x == 0) {
     st->d = d;
@@ -811,7 +862,8 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
   int rc = CHLL_OK;
   long long bw = B->wave_bytes;
   // Candidates: one wave or 48 MiB waves; each block size at its two highest
-  // occupancies (lower occupancies were never faster on this kernel).
+  // occupancies (lower occupancies were never faster on this kernel).  Trials
+  // measure every 10 sweeps like a production run.
   const long long kWaveOptions[] = {0ll, 48ll << 20};
   for (long long wb : kWaveOptions)
   for (int threads : {128, 256, 512}) {
@@ -830,7 +882,7 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
       rc = launch_batch(B, B->stream, 1, 0, 0);  // warm-up
       if (rc != CHLL_OK) break;
       cudaEventRecord(e0, B->stream);
-      rc = launch_batch(B, B->stream, trial_sweeps, 0, 0);
+      rc = launch_batch(B, B->stream, trial_sweeps, 10, 0);
       if (rc != CHLL_OK) break;
       cudaEventRecord(e1, B->stream);
       cudaError_t e = cudaEventSynchronize(e1);

@@ -154,6 +154,7 @@ struct chll_lattice {
   cudaStream_t stream = nullptr;
   std::vector<GraphEntry> graphs;
   uint64_t use_clock = 0;
+  int kernel = chll::kSweepAuto;
 
   LatticeView view() const {
     LatticeView v;
@@ -196,8 +197,9 @@ void drop_graphs(chll_lattice* L) {
   L->graphs.clear();
 }
 
-// Returns an executable graph of `nsweeps` steps (4 passes each) for this
-// coupling and key, capturing it on first use.
+// Returns an executable graph of `nsweeps` steps for this coupling and key,
+// capturing it on first use: 2 fused passes per step plus a closing flip
+// pass, or the reference's 4 half-sweeps per step.
 int get_graph(chll_lattice* L, const Coupling& cp, uint32_t k0, uint32_t k1, uint32_t rep,
               int nsweeps, cudaGraphExec_t* out) {
   for (auto& g : L->graphs) {
@@ -211,9 +213,19 @@ int get_graph(chll_lattice* L, const Coupling& cp, uint32_t k0, uint32_t k1, uin
   const LatticeView v = L->view();
   cudaGraph_t graph = nullptr;
   CHLL_CUDA_TRY(cudaStreamBeginCapture(L->capture_stream, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < nsweeps; ++s)
-    for (int p = 0; p < 4; ++p)
-      chll::launch_sweep_pass(v, cp, k0, k1, rep, L->ctl, p, L->capture_stream);
+  if (L->kernel == chll::kSweepAuto || L->kernel == chll::kSweepFused) {
+    // A0 B (A B)... F: the fused two-pass sweep, flips completed at the end
+    for (int s = 0; s < nsweeps; ++s) {
+      chll::launch_fused_pass(v, cp, k0, k1, rep, L->ctl, s ? chll::kFusedA : chll::kFusedA0,
+                              L->capture_stream);
+      chll::launch_fused_pass(v, cp, k0, k1, rep, L->ctl, chll::kFusedB, L->capture_stream);
+    }
+    chll::launch_fused_pass(v, cp, k0, k1, rep, L->ctl, chll::kFusedF, L->capture_stream);
+  } else {
+    for (int s = 0; s < nsweeps; ++s)
+      for (int p = 0; p < 4; ++p)
+        chll::launch_sweep_pass(v, cp, k0, k1, rep, L->ctl, p, L->capture_stream, L->kernel);
+  }
   cudaError_t e = cudaStreamEndCapture(L->capture_stream, &graph);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -646,6 +658,18 @@ void chll_lattice_destroy(chll_lattice* L) {
   delete L;
 }
 
+int chll_lattice_set_kernel(chll_lattice* L, int kernel) {
+  if (!L) return fail(CHLL_EINVAL, "null lattice");
+  if (kernel < 0 || kernel > 3)
+    return fail(CHLL_EINVAL, "set_kernel: kernel must be 0, 1, 2 or 3");
+  if (kernel == chll::kSweepStaged && !chll::staged_fits(L->view()))
+    return fail(CHLL_EINVAL, "set_kernel: rows of %d sites are too long for the staged kernel",
+                L->ni);
+  if (kernel != L->kernel) drop_graphs(L);
+  L->kernel = kernel;
+  return ok();
+}
+
 int chll_lattice_set_stream(chll_lattice* L, void* stream) {
   if (!L) return fail(CHLL_EINVAL, "null lattice");
   L->stream = stream ? (cudaStream_t)stream : L->own_stream;
@@ -755,10 +779,14 @@ int chll_lattice_sweep(chll_lattice* L, const chll_coupling* c, uint64_t seed, u
 int chll_lattice_pass(chll_lattice* L, const chll_coupling* c, uint64_t seed, uint32_t replica,
                       int pass) {
   if (!L || !c) return fail(CHLL_EINVAL, "pass: null argument");
-  if (pass < 0 || pass > 3) return fail(CHLL_EINVAL, "pass must be 0..3 (got %d)", pass);
+  if (pass < 0 || pass > 7) return fail(CHLL_EINVAL, "pass must be 0..7 (got %d)", pass);
   if (!(c->kT >= 0.0)) return fail(CHLL_EINVAL, "pass: kT must be >= 0");
-  chll::launch_sweep_pass(L->view(), make_coupling(*c), seed_lo(seed), seed_hi(seed), replica,
-                          L->ctl, pass, L->stream);
+  if (pass >= 4)
+    chll::launch_fused_pass(L->view(), make_coupling(*c), seed_lo(seed), seed_hi(seed), replica,
+                            L->ctl, pass - 4, L->stream);
+  else
+    chll::launch_sweep_pass(L->view(), make_coupling(*c), seed_lo(seed), seed_hi(seed),
+                            replica, L->ctl, pass, L->stream, L->kernel);
   CHLL_CUDA_TRY(cudaGetLastError());
   return ok();
 }

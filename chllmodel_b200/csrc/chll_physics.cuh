@@ -14,14 +14,6 @@ struct Nbrs {
   float4 b[6];
 };
 
-// (v x b) . e_axis for axis 0,1,2 (chll_mod.f90:373,387,401).
-template <int AXIS>
-__device__ __forceinline__ float cross_axis(float vx, float vy, float vz, float4 b) {
-  if (AXIS == 0) return vy * b.z - vz * b.y;
-  if (AXIS == 1) return vz * b.x - vx * b.z;
-  return vx * b.y - vy * b.x;
-}
-
 // Director proposal of chll_mod.f90:149-182: rotate n in its tangent plane by
 // amplitude d at angle phi = 2*pi*u, then renormalise.  |nz| > 0.999 (FP64 in
 // the reference) is exactly |nz| >= 0.999f for an FP32 nz.
@@ -31,86 +23,158 @@ __device__ __forceinline__ float cross_axis(float vx, float vy, float vz, float4
 __device__ __forceinline__ void propose_director(float nx, float ny, float nz, float d, float u,
                                                  float& mx, float& my, float& mz) {
   float sn, cs;
-  __sincosf(6.28318530717958647692f * (u - 0.5f), &sn, &cs);
-  sn = -sn;
-  cs = -cs;
+  __sincosf(__fmul_rn(6.28318530717958647692f, u - 0.5f), &sn, &cs);
+  const float a = -__fmul_rn(d, cs), bb = -__fmul_rn(d, sn);  // d cos(phi), d sin(phi)
   float x, y, z;
   if (fabsf(nz) >= 0.999f) {
-    x = nx + d * cs;
-    y = ny + d * sn;
+    x = __fadd_rn(nx, a);
+    y = __fadd_rn(ny, bb);
     z = nz;
   } else {
-    const float ru = rsqrtf(nx * nx + ny * ny);
-    const float ux = -ny * ru, uy = nx * ru;
-    float vx = -nz * nx, vy = -nz * ny, vz = nx * nx + ny * ny;
-    const float rv = rsqrtf(vx * vx + vy * vy + vz * vz);
-    vx *= rv;
-    vy *= rv;
-    vz *= rv;
-    const float a = d * cs, bb = d * sn;
-    x = nx + a * ux + bb * vx;
-    y = ny + a * uy + bb * vy;
-    z = nz + bb * vz;
+    const float rho2 = fmaf(ny, ny, __fmul_rn(nx, nx));
+    const float ru = rsqrtf(rho2);
+    const float ux = -__fmul_rn(ny, ru), uy = __fmul_rn(nx, ru);
+    float vx = -__fmul_rn(nz, nx), vy = -__fmul_rn(nz, ny), vz = rho2;
+    const float rv = rsqrtf(fmaf(vz, vz, fmaf(vy, vy, __fmul_rn(vx, vx))));
+    vx = __fmul_rn(vx, rv);
+    vy = __fmul_rn(vy, rv);
+    vz = __fmul_rn(vz, rv);
+    x = fmaf(bb, vx, fmaf(a, ux, nx));
+    y = fmaf(bb, vy, fmaf(a, uy, ny));
+    z = fmaf(bb, vz, nz);
   }
-  const float r = rsqrtf(x * x + y * y + z * z);
-  mx = x * r;
-  my = y * r;
-  mz = z * r;
+  const float r = rsqrtf(fmaf(z, z, fmaf(y, y, __fmul_rn(x, x))));
+  mx = __fmul_rn(x, r);
+  my = __fmul_rn(y, r);
+  mz = __fmul_rn(z, r);
 }
 
-// One bond's contribution to E(m) - E(n) for a director trial n -> m: the
-// nematic part into dn, and (s + s_b)*(dot_m*x_m - dot_o*x_o) into the
-// accumulator of its direction (+axis bonds carry sigma = -1, -axis +1).
+// Every product and sum below is an explicit fmaf / __fmul_rn / __fadd_rn, so
+// the compiler cannot contract it differently in different kernels: the
+// plain, fused, staged and batched sweeps compute identical bits.
+
+// v . b
+__device__ __forceinline__ float dot3(float vx, float vy, float vz, float4 b) {
+  return fmaf(vz, b.z, fmaf(vy, b.y, __fmul_rn(vx, b.x)));
+}
+
+// (v x b) . e_axis for axis 0,1,2 (chll_mod.f90:373,387,401).
 template <int AXIS>
-__device__ __forceinline__ void dir_bond(float nx, float ny, float nz, float mx, float my,
-                                         float mz, float s, float4 b, float& dn, float& dc) {
-  const float d_o = nx * b.x + ny * b.y + nz * b.z;
-  const float d_m = mx * b.x + my * b.y + mz * b.z;
-  const float x_o = cross_axis<AXIS>(nx, ny, nz, b);
-  const float x_m = cross_axis<AXIS>(mx, my, mz, b);
-  dn = fmaf(d_o, d_o, dn);
-  dn = fmaf(-d_m, d_m, dn);
-  dc = fmaf(s + b.w, fmaf(d_m, x_m, -d_o * x_o), dc);
+__device__ __forceinline__ float cross_axis(float vx, float vy, float vz, float4 b) {
+  if (AXIS == 0) return fmaf(vy, b.z, -__fmul_rn(vz, b.y));
+  if (AXIS == 1) return fmaf(vz, b.x, -__fmul_rn(vx, b.z));
+  return fmaf(vx, b.y, -__fmul_rn(vy, b.x));
 }
 
-// Energy difference of the director trial: eps*sum(dot_o^2 - dot_m^2) +
-// K*sum(sigma*sfac*(dot_m*x_m - dot_o*x_o)), sfac = (s + s_b)/2.
-__device__ __forceinline__ float director_dE(const float4& n, float mx, float my, float mz,
-                                             const Nbrs& nb, const Coupling& cp) {
-  float dn = 0.f, dplus = 0.f, dminus = 0.f;
-  dir_bond<0>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[0], dn, dplus);
-  dir_bond<0>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[1], dn, dminus);
-  dir_bond<1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[2], dn, dplus);
-  dir_bond<1>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[3], dn, dminus);
-  dir_bond<2>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[4], dn, dplus);
-  dir_bond<2>(n.x, n.y, n.z, mx, my, mz, n.w, nb.b[5], dn, dminus);
-  return fmaf(cp.eps, dn, 0.5f * cp.K * (dminus - dplus));
-}
+// Bond sums of one director v over its six neighbours b, with
+// p_b = (v.b) * ((v x b).e_b) and sigma_b = -1 for +axis, +1 for -axis:
+//   q = sum (v.b)^2,   c = sum sigma_b p_b,   w = sum sigma_b s_b p_b.
+// The local energy (chll_mod.f90:363-412) is then
+//   E(v, s) = sum_b eps (1 - (v.b)^2) + (K/2) (s c + w) - g s,
+// so a director trial and a chirality flip both follow from q, c, w of the
+// current and the trial director.
+struct BondSums {
+  float q, c, w;
+};
 
 template <int AXIS, int SIGMA>
-__device__ __forceinline__ float chiral_bond(const float4& n, float4 b) {
-  const float dt = n.x * b.x + n.y * b.y + n.z * b.z;
-  return (float)SIGMA * dt * cross_axis<AXIS>(n.x, n.y, n.z, b);
+__device__ __forceinline__ void bond_acc(float vx, float vy, float vz, float4 b, BondSums& S) {
+  const float dt = dot3(vx, vy, vz, b);
+  const float p = __fmul_rn(dt, cross_axis<AXIS>(vx, vy, vz, b));
+  S.q = fmaf(dt, dt, S.q);
+  S.c = SIGMA > 0 ? __fadd_rn(S.c, p) : __fsub_rn(S.c, p);
+  S.w = fmaf(SIGMA > 0 ? b.w : -b.w, p, S.w);
 }
 
-// Energy difference of the chirality flip s -> -s (chll_mod.f90:226-233):
-// the nematic terms cancel and (snew + s_b)/2 - (s + s_b)/2 = -s, so
-//   dE = -s*K*sum(sigma*dot*cross) + 2*g*s.
-__device__ __forceinline__ float spin_dE(const float4& n, const Nbrs& nb, const Coupling& cp) {
-  float c = chiral_bond<0, -1>(n, nb.b[0]);
-  c += chiral_bond<0, +1>(n, nb.b[1]);
-  c += chiral_bond<1, -1>(n, nb.b[2]);
-  c += chiral_bond<1, +1>(n, nb.b[3]);
-  c += chiral_bond<2, -1>(n, nb.b[4]);
-  c += chiral_bond<2, +1>(n, nb.b[5]);
-  return n.w * fmaf(-cp.K, c, 2.0f * cp.g);
+__device__ __forceinline__ BondSums bond_sums(float vx, float vy, float vz, const Nbrs& nb) {
+  BondSums S = {0.f, 0.f, 0.f};
+  bond_acc<0, -1>(vx, vy, vz, nb.b[0], S);
+  bond_acc<0, +1>(vx, vy, vz, nb.b[1], S);
+  bond_acc<1, -1>(vx, vy, vz, nb.b[2], S);
+  bond_acc<1, +1>(vx, vy, vz, nb.b[3], S);
+  bond_acc<2, -1>(vx, vy, vz, nb.b[4], S);
+  bond_acc<2, +1>(vx, vy, vz, nb.b[5], S);
+  return S;
+}
+
+// E(m, s) - E(n, s) = eps (q_n - q_m) + (K/2) (s (c_m - c_n) + (w_m - w_n)).
+__device__ __forceinline__ float director_dE(const BondSums& o, const BondSums& m, float s,
+                                             const Coupling& cp) {
+  const float chi = fmaf(s, __fsub_rn(m.c, o.c), __fsub_rn(m.w, o.w));
+  return fmaf(cp.eps, __fsub_rn(o.q, m.q), __fmul_rn(__fmul_rn(0.5f, cp.K), chi));
+}
+
+// E(n, -s) - E(n, s) = s (2 g - K c) (chll_mod.f90:226-233): the flip does not
+// depend on the neighbours' chiralities, only on c of the current director.
+__device__ __forceinline__ float flip_dE(float c, float s, const Coupling& cp) {
+  return __fmul_rn(s, fmaf(-cp.K, c, __fmul_rn(2.0f, cp.g)));
 }
 
 // Metropolis rule of chll_mod.f90:188-200: accept if dE < 0, else if
 // u <= exp(-dE/kT).  At kT = 0 this gives exp(-inf) = 0 for dE > 0 and NaN
 // (reject) for dE = 0, as the reference's division does.
 __device__ __forceinline__ bool metropolis(float dE, float u, float inv_kT) {
-  return (dE < 0.f) || (u <= __expf(-dE * inv_kT));
+  return (dE < 0.f) || (u <= __expf(__fmul_rn(-dE, inv_kT)));
+}
+
+// The trials of one site of a work unit, in chain order: the chirality flip
+// left over from the previous sweep (FLIP_BEFORE, uniform ub), the director
+// trial of this sweep (DIR, uniforms ua for the angle and uacc for the
+// acceptance), the chirality flip of this sweep (FLIP_AFTER, uniform uf).
+// The bond sums of the current director serve the flip and the director
+// trial; after an accepted trial those of the trial director serve the
+// second flip, exactly as a separate flip pass would recompute them.
+template <bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
+__device__ __forceinline__ void site_trials(float4& n, const Nbrs& nb, float d, const Coupling& cp,
+                                            float ub, float ua, float uacc, float uf,
+                                            unsigned int& nacc, unsigned int& nflip) {
+  BondSums o = bond_sums(n.x, n.y, n.z, nb);
+  if (FLIP_BEFORE) {
+    if (metropolis(flip_dE(o.c, n.w, cp), ub, cp.inv_kT)) {
+      n.w = -n.w;
+      ++nflip;
+    }
+  }
+  if (DIR) {
+    float mx, my, mz;
+    propose_director(n.x, n.y, n.z, d, ua, mx, my, mz);
+    const BondSums m = bond_sums(mx, my, mz, nb);
+    if (metropolis(director_dE(o, m, n.w, cp), uacc, cp.inv_kT)) {
+      n.x = mx;
+      n.y = my;
+      n.z = mz;
+      if (FLIP_AFTER) o = m;
+      ++nacc;
+    }
+  }
+  if (FLIP_AFTER) {
+    if (metropolis(flip_dE(o.c, n.w, cp), uf, cp.inv_kT)) {
+      n.w = -n.w;
+      ++nflip;
+    }
+  }
+}
+
+// Both sites of unit g of colour C (sites present: v0, v1).  Counters:
+// the previous sweep's flips {g, step-1, replica, 2+C} (words 0, 2), the
+// director trials {g, step, replica, C} (words 0,1 and 2,3), this sweep's
+// flips {g, step, replica, 2+C} (words 0, 2).
+template <int C, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
+__device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& nb0,
+                                            const Nbrs& nb1, bool v0, bool v1, uint32_t g,
+                                            uint32_t step, float d, const Coupling& cp,
+                                            uint32_t key0, uint32_t key1, uint32_t replica,
+                                            unsigned int& nacc, unsigned int& nflip) {
+  Ctr4 rb = {{0u, 0u, 0u, 0u}}, rd = {{0u, 0u, 0u, 0u}}, rf = {{0u, 0u, 0u, 0u}};
+  if (FLIP_BEFORE) rb = philox4x32_10({{g, step - 1u, replica, 2u + (uint32_t)C}}, key0, key1);
+  if (DIR) rd = philox4x32_10({{g, step, replica, (uint32_t)C}}, key0, key1);
+  if (FLIP_AFTER) rf = philox4x32_10({{g, step, replica, 2u + (uint32_t)C}}, key0, key1);
+  if (v0)
+    site_trials<FLIP_BEFORE, DIR, FLIP_AFTER>(n0, nb0, d, cp, u01(rb.v[0]), u01(rd.v[0]),
+                                              u01(rd.v[1]), u01(rf.v[0]), nacc, nflip);
+  if (v1)
+    site_trials<FLIP_BEFORE, DIR, FLIP_AFTER>(n1, nb1, d, cp, u01(rb.v[2]), u01(rd.v[2]),
+                                              u01(rd.v[3]), u01(rf.v[2]), nacc, nflip);
 }
 
 }  // namespace chll

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "chll_common.cuh"
+#include "staged.cuh"
 #include "sweep.cuh"
 #include "sweep_unit.cuh"
 
@@ -29,21 +30,14 @@ namespace chll {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before a stage counts as lost
 
-template <bool DIRECTOR, int C, bool PERIODIC>
-__global__ void __launch_bounds__(kThreads, 3)
-    sweep_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, uint32_t key0, uint32_t key1,
-                      uint32_t replica, Control* __restrict__ ctl) {
-  const long long step = ctl->step;
-  const float d = (float)ctl->d;
-  unsigned int accepted = 0;
-  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
-       g += gridDim.x * kThreads) {
-    accepted += sweep_unit<DIRECTOR, C, PERIODIC>(L, G, g, (uint32_t)step, d, cp, key0, key1,
-                                                  replica);
-  }
-
-  // CTA-aggregated accept count, then the last-CTA epilogue.
+// CTA-aggregated accept count, then the step epilogue in the last CTA to
+// finish (paccept and d after the second director pass, faccept and the step
+// increment after the second flip pass; chll_mod.f90:83-93).
+template <bool DIRECTOR, int C>
+__device__ __forceinline__ void pass_epilogue(Control* __restrict__ ctl, unsigned int accepted,
+                                              long long step) {
   __shared__ unsigned int s_cnt;
   __shared__ bool s_last;
   const int tid = threadIdx.x;
@@ -84,10 +78,135 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
 }
 
-// Resident CTAs per SM of each pass kernel and the SM count, queried once
-// per device (outside any stream capture; see sweep_prepare).
+// Direct kernel: every unit loads its neighbours from global memory (L1/L2).
+template <bool DIRECTOR, int C, bool PERIODIC>
+__global__ void __launch_bounds__(kThreads, 3)
+    sweep_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, uint32_t key0, uint32_t key1,
+                      uint32_t replica, Control* __restrict__ ctl) {
+  const long long step = ctl->step;
+  const float d = (float)ctl->d;
+  unsigned int accepted = 0;
+  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
+       g += gridDim.x * kThreads) {
+    accepted += sweep_unit<DIRECTOR, C, PERIODIC>(L, G, g, (uint32_t)step, d, cp, key0, key1,
+                                                  replica);
+  }
+  pass_epilogue<DIRECTOR, C>(ctl, accepted, step);
+}
+
+// Fused sweep: a sweep in two passes instead of four.  A flip's energy
+// difference depends on the site's director and its neighbours' directors
+// but not on their chiralities, and the directors do not change during the
+// flip passes, so
+//   pass A (colour 0): the previous sweep's colour-0 flips, then this
+//                      sweep's colour-0 director trials,
+//   pass B (colour 1): this sweep's colour-1 director trials, then its
+//                      colour-1 flips,
+// with a colour-0 flip pass (F) after the last sweep, give the chain of the
+// four half-sweeps D0 D1 F0 F1 per sweep exactly: every trial sees the same
+// state and draws the same counter.  Each site is read and written once per
+// pass, so a sweep moves half the bytes of the four-pass form.
+//
+// Control epilogue (last CTA): B closes the director count (paccept, d) and
+// advances the step; A and F close the previous sweep's flip count
+// (faccept), which B started with the colour-1 flips.
+template <int PHASE>
+__device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsigned int nacc,
+                                               unsigned int nflip, long long step) {
+  constexpr bool DIR = PHASE != kFusedF;
+  constexpr bool FLIPS = PHASE != kFusedA0;
+  __shared__ unsigned int s_cnt[2];
+  __shared__ bool s_last;
+  const int tid = threadIdx.x;
+  if (tid < 2) s_cnt[tid] = 0;
+  __syncthreads();
+  if (DIR) {
+    const unsigned int w = __reduce_add_sync(0xffffffffu, nacc);
+    if ((tid & 31) == 0 && w) atomicAdd(&s_cnt[0], w);
+  }
+  if (FLIPS) {
+    const unsigned int w = __reduce_add_sync(0xffffffffu, nflip);
+    if ((tid & 31) == 0 && w) atomicAdd(&s_cnt[1], w);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (DIR && s_cnt[0]) atomicAdd(&ctl->nacc, (unsigned long long)s_cnt[0]);
+    if (FLIPS && s_cnt[1]) atomicAdd(&ctl->nflip, (unsigned long long)s_cnt[1]);
+    __threadfence();
+    const unsigned int ticket = atomicAdd(&ctl->done, 1u);
+    s_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last && tid == 0) {
+    __threadfence();
+    ctl->done = 0;
+    const float n3 = (float)ctl->nsites;
+    if (PHASE == kFusedB) {
+      const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
+      const float pa = (float)na / n3;  // chll_mod.f90:83
+      ctl->paccept = pa;
+      ctl->nacc_last = (long long)na;
+      ctl->nacc = 0;
+      if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
+      ctl->step = step + 1;
+    } else if (PHASE == kFusedA || PHASE == kFusedF) {
+      const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
+      ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
+      ctl->nflip_last = (long long)nf;
+      ctl->nflip = 0;
+    }
+  }
+}
+
+template <int PHASE, bool PERIODIC>
+__global__ void __launch_bounds__(kThreads, 3)
+    fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, uint32_t key0, uint32_t key1,
+                      uint32_t replica, Control* __restrict__ ctl) {
+  constexpr int C = PHASE == kFusedB ? 1 : 0;
+  constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
+  constexpr bool DIR = PHASE != kFusedF;
+  constexpr bool FLIP_AFTER = PHASE == kFusedB;
+  const long long step = ctl->step;
+  const float d = (float)ctl->d;
+  unsigned int nacc = 0, nflip = 0;
+  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
+       g += gridDim.x * kThreads) {
+    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, key0,
+                                                         key1, replica, nacc, nflip);
+  }
+  fused_epilogue<PHASE>(ctl, nacc, nflip, step);
+}
+
+// Staged kernel: row tiles come into shared memory by bulk copies one tile
+// ahead of the compute (staged.cuh).  Same chain as the direct kernel.
+template <bool DIRECTOR, int C, bool PERIODIC>
+__global__ void __launch_bounds__(kThreads, 2)
+    staged_pass_kernel(LatticeView L, TileGeom T, Coupling cp, uint32_t key0, uint32_t key1,
+                       uint32_t replica, Control* __restrict__ ctl) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  if (threadIdx.x == 0) {
+    mbar_init(smem_addr(&bars[0]), 1);
+    mbar_init(smem_addr(&bars[1]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const long long step = ctl->step;
+  const float d = (float)ctl->d;
+  uint32_t uses0 = 0, uses1 = 0;
+  bool timed_out = false;
+  const unsigned int accepted = staged_pass<DIRECTOR, C, PERIODIC>(
+      T, L, reinterpret_cast<float4*>(smem), smem_addr(&bars[0]), smem_addr(&bars[1]), uses0,
+      uses1, blockIdx.x, gridDim.x, (uint32_t)step, d, cp, key0, key1, replica, kWaitLimit,
+      &timed_out);
+  if (timed_out && threadIdx.x == 0) atomicOr(&ctl->status, 2u);
+  pass_epilogue<DIRECTOR, C>(ctl, accepted, step);
+}
+
 using PassKernel = void (*)(LatticeView, SweepGeom, Coupling, uint32_t, uint32_t, uint32_t,
                            Control*);
+using StagedKernel = void (*)(LatticeView, TileGeom, Coupling, uint32_t, uint32_t, uint32_t,
+                             Control*);
 
 // [periodic][pass]
 const PassKernel kKernels[2][4] = {
@@ -95,10 +214,31 @@ const PassKernel kKernels[2][4] = {
      sweep_pass_kernel<false, 0, false>, sweep_pass_kernel<false, 1, false>},
     {sweep_pass_kernel<true, 0, true>, sweep_pass_kernel<true, 1, true>,
      sweep_pass_kernel<false, 0, true>, sweep_pass_kernel<false, 1, true>}};
+const StagedKernel kStaged[2][4] = {
+    {staged_pass_kernel<true, 0, false>, staged_pass_kernel<true, 1, false>,
+     staged_pass_kernel<false, 0, false>, staged_pass_kernel<false, 1, false>},
+    {staged_pass_kernel<true, 0, true>, staged_pass_kernel<true, 1, true>,
+     staged_pass_kernel<false, 0, true>, staged_pass_kernel<false, 1, true>}};
 
+// [periodic][phase]
+const PassKernel kFused[2][4] = {
+    {fused_pass_kernel<kFusedA0, false>, fused_pass_kernel<kFusedA, false>,
+     fused_pass_kernel<kFusedB, false>, fused_pass_kernel<kFusedF, false>},
+    {fused_pass_kernel<kFusedA0, true>, fused_pass_kernel<kFusedA, true>,
+     fused_pass_kernel<kFusedB, true>, fused_pass_kernel<kFusedF, true>}};
+
+// Largest dynamic shared memory a staged CTA may ask for (2 stages).
+constexpr size_t kStagedSmemMax = 200 * 1024;
+
+// Resident CTAs per SM of each pass kernel and the SM count, queried once
+// per device (outside any stream capture; see sweep_prepare).  Staged
+// kernels are queried per shared-memory size on first use of that size.
 struct DeviceShape {
   int sms = 0;
   int per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  int fused_per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  size_t staged_smem[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last size asked per kernel
+  int staged_per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 std::mutex g_shape_mutex;
 DeviceShape g_shape[64];
@@ -109,7 +249,7 @@ int occupancy(PassKernel k) {
   return n > 0 ? n : 1;
 }
 
-const DeviceShape& device_shape() {
+DeviceShape& device_shape() {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
@@ -119,24 +259,79 @@ const DeviceShape& device_shape() {
     cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
     if (s.sms <= 0) s.sms = 148;
     for (int per = 0; per < 2; ++per)
-      for (int p = 0; p < 4; ++p) s.per_sm[per][p] = occupancy(kKernels[per][p]);
+      for (int p = 0; p < 4; ++p) {
+        s.per_sm[per][p] = occupancy(kKernels[per][p]);
+        s.fused_per_sm[per][p] = occupancy(kFused[per][p]);
+        cudaFuncSetAttribute(kStaged[per][p], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kStagedSmemMax);
+      }
   }
   return s;
+}
+
+int staged_occupancy(DeviceShape& ds, int per, int pass, size_t smem) {
+  std::lock_guard<std::mutex> lk(g_shape_mutex);
+  const int idx = per * 4 + pass;
+  if (ds.staged_smem[idx] != smem) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kStaged[per][pass], kThreads, smem);
+    ds.staged_smem[idx] = smem;
+    ds.staged_per_sm[idx] = n > 0 ? n : 1;
+  }
+  return ds.staged_per_sm[idx];
 }
 
 }  // namespace
 
 void sweep_prepare() { (void)device_shape(); }
 
+// Rows per tile of the staged kernel: about one unit per thread.
+uint32_t staged_rows(const LatticeView& L) {
+  const uint32_t Q = (uint32_t)(L.hx >> 1);
+  uint32_t R = Q ? kThreads / Q : 1;
+  if (R < 1) R = 1;
+  if (R > (uint32_t)L.nj) R = (uint32_t)L.nj;
+  return R;
+}
+
+size_t staged_smem_bytes(const LatticeView& L) {
+  const uint32_t R = staged_rows(L);
+  return 2 * (size_t)(4 * R + 2) * (size_t)L.hx * sizeof(float4);
+}
+
+bool staged_fits(const LatticeView& L) {
+  return staged_smem_bytes(L) <= kStagedSmemMax && (uint32_t)(L.hx >> 1) <= 4 * kThreads;
+}
+
 void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
-                       uint32_t replica, Control* ctl, int pass, cudaStream_t stream) {
-  const DeviceShape& ds = device_shape();
+                       uint32_t replica, Control* ctl, int pass, cudaStream_t stream,
+                       int kernel) {
+  DeviceShape& ds = device_shape();
+  const int per = L.periodic ? 1 : 0;
+  if (kernel == kSweepStaged && staged_fits(L)) {
+    const TileGeom T = make_tile_geom(L, staged_rows(L));
+    const size_t smem = staged_smem_bytes(L);
+    const uint32_t resident = (uint32_t)ds.sms * (uint32_t)staged_occupancy(ds, per, pass & 3, smem);
+    const dim3 grid(T.ntiles < resident ? (T.ntiles ? T.ntiles : 1) : resident);
+    kStaged[per][pass & 3]<<<grid, kThreads, smem, stream>>>(L, T, cp, key0, key1, replica, ctl);
+    return;
+  }
   const SweepGeom G = make_geom(L);
   const uint32_t need = (G.units + kThreads - 1) / kThreads;
-  const int per = L.periodic ? 1 : 0;
   const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.per_sm[per][pass & 3];
   const dim3 grid(need < resident ? (need ? need : 1) : resident);
   kKernels[per][pass & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
+}
+
+void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
+                       uint32_t replica, Control* ctl, int phase, cudaStream_t stream) {
+  DeviceShape& ds = device_shape();
+  const int per = L.periodic ? 1 : 0;
+  const SweepGeom G = make_geom(L);
+  const uint32_t need = (G.units + kThreads - 1) / kThreads;
+  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[per][phase & 3];
+  const dim3 grid(need < resident ? (need ? need : 1) : resident);
+  kFused[per][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
 }
 
 }  // namespace chll

@@ -9,8 +9,22 @@ namespace chll {
 // sweep.cu: per-device launch shapes (call once per device, outside any
 // stream capture) and one half-sweep (pass = kPassDir0..kPassSpin1).
 void sweep_prepare();
+// Sweep form: the two-pass fused sweep (auto), or the reference's four
+// half-sweeps with the direct kernel or the staged kernel (shared-memory
+// tiles by bulk copies).  All give the same chain.  Single half-sweeps
+// (chll_lattice_pass) use the direct kernel unless staged is chosen.
+enum SweepKernel : int { kSweepAuto = 0, kSweepDirect = 1, kSweepStaged = 2, kSweepFused = 3 };
 void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
-                       uint32_t replica, Control* ctl, int pass, cudaStream_t stream);
+                       uint32_t replica, Control* ctl, int pass, cudaStream_t stream,
+                       int kernel = kSweepAuto);
+bool staged_fits(const LatticeView& L);
+// Fused sweep passes (sweep.cu): A0 = director trials of colour 0 (first
+// sweep), A = previous sweep's colour-0 flips + colour-0 director trials,
+// B = colour-1 director trials + colour-1 flips (ends the sweep),
+// F = previous sweep's colour-0 flips (after the last sweep).
+enum FusedPhase : int { kFusedA0 = 0, kFusedA = 1, kFusedB = 2, kFusedF = 3 };
+void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
+                       uint32_t replica, Control* ctl, int phase, cudaStream_t stream);
 
 // layout.cu: natural-order (F-order, i fastest) <-> red/black float4.
 void launch_pack_f64(const LatticeView& L, const double* nx, const double* ny, const double* nz,

@@ -33,13 +33,14 @@ __host__ inline SweepGeom make_geom(const LatticeView& L) {
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
-// Updates unit g in place; returns the number of accepted trials (0..2).
-template <bool DIRECTOR, int C, bool PERIODIC>
-__device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const SweepGeom& G,
-                                                   uint32_t g, uint32_t step, float d,
-                                                   const Coupling& cp, uint32_t key0,
-                                                   uint32_t key1, uint32_t replica) {
-  constexpr uint32_t kPass = (DIRECTOR ? 0u : 2u) + (uint32_t)C;
+// Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
+// unit_trials (chll_physics.cuh), adding accepted director trials to nacc
+// and accepted flips to nflip.
+template <int C, bool PERIODIC, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
+__device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
+                                          uint32_t step, float d, const Coupling& cp,
+                                          uint32_t key0, uint32_t key1, uint32_t replica,
+                                          unsigned int& nacc, unsigned int& nflip) {
   const uint32_t hx = (uint32_t)L.hx;
   const uint32_t nj = (uint32_t)L.nj, nk = (uint32_t)L.nk, ni = (uint32_t)L.ni;
   const uint32_t plane = hx * nj;
@@ -95,52 +96,23 @@ __device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const S
   nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
   nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
 
-  Ctr4 ctr = {{g, step, replica, kPass}};
-  const Ctr4 r = philox4x32_10(ctr, key0, key1);
-
-  unsigned int accepted = 0;
-  if (DIRECTOR) {
-    if (v0) {
-      float mx, my, mz;
-      propose_director(n0.x, n0.y, n0.z, d, u01(r.v[0]), mx, my, mz);
-      const float dE = director_dE(n0, mx, my, mz, nb0, cp);
-      if (metropolis(dE, u01(r.v[1]), cp.inv_kT)) {
-        n0.x = mx;
-        n0.y = my;
-        n0.z = mz;
-        ++accepted;
-      }
-    }
-    if (v1) {
-      float mx, my, mz;
-      propose_director(n1.x, n1.y, n1.z, d, u01(r.v[2]), mx, my, mz);
-      const float dE = director_dE(n1, mx, my, mz, nb1, cp);
-      if (metropolis(dE, u01(r.v[3]), cp.inv_kT)) {
-        n1.x = mx;
-        n1.y = my;
-        n1.z = mz;
-        ++accepted;
-      }
-    }
-  } else {
-    if (v0) {
-      const float dE = spin_dE(n0, nb0, cp);
-      if (metropolis(dE, u01(r.v[0]), cp.inv_kT)) {
-        n0.w = -n0.w;
-        ++accepted;
-      }
-    }
-    if (v1) {
-      const float dE = spin_dE(n1, nb1, cp);
-      if (metropolis(dE, u01(r.v[2]), cp.inv_kT)) {
-        n1.w = -n1.w;
-        ++accepted;
-      }
-    }
-  }
+  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp, key0,
+                                               key1, replica, nacc, nflip);
   cen[0] = n0;
   cen[1] = n1;
-  return accepted;
+}
+
+// One of the reference's four half-sweeps on unit g; returns the number of
+// accepted trials (0..2).
+template <bool DIRECTOR, int C, bool PERIODIC>
+__device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const SweepGeom& G,
+                                                   uint32_t g, uint32_t step, float d,
+                                                   const Coupling& cp, uint32_t key0,
+                                                   uint32_t key1, uint32_t replica) {
+  unsigned int nacc = 0, nflip = 0;
+  unit_step<C, PERIODIC, false, DIRECTOR, !DIRECTOR>(L, G, g, step, d, cp, key0, key1, replica,
+                                                     nacc, nflip);
+  return DIRECTOR ? nacc : nflip;
 }
 
 // The reference's step-size rule (chll_mod.f90:83-90): paccept is an FP32

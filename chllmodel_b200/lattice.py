@@ -19,6 +19,10 @@ def coupling(kT: float, K: float, g: float = 0.0, eps: float = 1.0) -> Coupling:
     return Coupling(float(kT), float(K), float(g), float(eps))
 
 
+# chll_lattice_pass codes of the fused sweep's passes
+FUSED_A0, FUSED_A, FUSED_B, FUSED_F = 4, 5, 6, 7
+
+
 class Lattice:
     """One ni x nj x nk lattice on the GPU (boundary 'open' or 'periodic')."""
 
@@ -63,6 +67,14 @@ class Lattice:
     # -- state ------------------------------------------------------------
     def set_stream(self, stream_ptr: int | None) -> None:
         check(self._L.chll_lattice_set_stream(self._h, ct.c_void_p(stream_ptr or 0)))
+
+    def set_kernel(self, kind: str) -> None:
+        """Sweep form: 'auto' (= 'fused'), 'fused' (two passes per sweep),
+        'direct' (the reference's four half-sweeps, neighbours from global
+        memory) or 'staged' (four half-sweeps from shared-memory row tiles).
+        All give the same chain bit for bit."""
+        code = {"auto": 0, "direct": 1, "staged": 2, "fused": 3}[kind]
+        check(self._L.chll_lattice_set_kernel(self._h, code))
 
     def sync(self) -> None:
         check(self._L.chll_lattice_sync(self._h))
@@ -128,6 +140,9 @@ class Lattice:
                                          int(nsweeps)))
 
     def half_sweep(self, cp: Coupling, p: int, seed: int = 1, replica: int = 0) -> None:
+        """One pass: 0-3 the reference's half-sweeps (director colour 0/1,
+        chirality colour 0/1); FUSED_A0 / FUSED_A / FUSED_B / FUSED_F the
+        fused sweep's passes (steps: A0 B (A B)... F)."""
         check(self._L.chll_lattice_pass(self._h, ct.byref(cp), int(seed), int(replica), int(p)))
 
     def reserve_rows(self, n: int) -> None:

@@ -131,6 +131,14 @@ void chll_lattice_destroy(chll_lattice* lat);
  * the lattice's own stream; cudaStreamLegacy (0x1) selects the legacy default
  * stream). */
 int chll_lattice_set_stream(chll_lattice* lat, void* stream);
+/* Sweep form: 0 auto (= 3), 1 the reference's four half-sweeps per step with
+ * neighbours read from global memory, 2 the four half-sweeps with row tiles
+ * staged in shared memory by bulk copies, 3 the fused two-pass sweep (each
+ * pass reads and writes every site once; the colour-0 flips of a step run at
+ * the start of the next step's first pass, and after the last step).  All give
+ * the same chain bit for bit.  chll_lattice_pass runs the staged kernel under
+ * 2 and the direct kernel otherwise. */
+int chll_lattice_set_kernel(chll_lattice* lat, int kernel);
 int chll_lattice_sync(chll_lattice* lat);
 /* Random initial state: directors uniform on the sphere, s = +-1 with p=1/2. */
 int chll_lattice_init_random(chll_lattice* lat, uint64_t seed, uint32_t replica);
@@ -148,11 +156,17 @@ int chll_lattice_storage(chll_lattice* lat, void** colour0, void** colour1, int6
 int chll_lattice_set_control(chll_lattice* lat, double d, int64_t step, int64_t adapt_until);
 int chll_lattice_get_control(chll_lattice* lat, double* d, int64_t* step, double* paccept,
                              double* faccept);
-/* nsweeps full steps (4 half-sweeps each) from the control block's step.
- * Consecutive calls with the same count replay one captured CUDA graph. */
+/* nsweeps full steps from the control block's step, in the form chosen by
+ * chll_lattice_set_kernel; every call ends with all trials of its last step
+ * done.  Consecutive calls with the same count replay one captured CUDA graph. */
 int chll_lattice_sweep(chll_lattice* lat, const chll_coupling* c, uint64_t seed,
                        uint32_t replica, int nsweeps);
-/* One half-sweep: pass 0/1 director colour 0/1, 2/3 chirality colour 0/1. */
+/* One pass.  The reference's half-sweeps: 0/1 director trials on colour 0/1,
+ * 2/3 chirality flips on colour 0/1 (a step is 0,1,2,3).  The fused passes:
+ * 4 colour-0 director trials (first step), 5 the previous step's colour-0
+ * flips + colour-0 director trials, 6 colour-1 director trials + colour-1
+ * flips (ends the step), 7 the previous step's colour-0 flips (closes the last
+ * step): steps t..t+n-1 are 4,6, then 5,6 n-1 times, then 7. */
 int chll_lattice_pass(chll_lattice* lat, const chll_coupling* c, uint64_t seed,
                       uint32_t replica, int pass);
 /* Device measurement rows: reserve room for n rows, enqueue the FP64

@@ -204,3 +204,40 @@ def test_graph_replay_equals_single_passes(oracle):
     assert a.control() == b.control()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("shape,periodic", [((16, 16, 16), True), ((24, 10, 6), False),
+                                            ((7, 9, 5), False), ((6, 4, 8), True),
+                                            ((120, 6, 4), True), ((64, 64, 4), False)])
+def test_sweep_forms_follow_one_chain(shape, periodic):
+    """The fused two-pass sweep, the four half-sweeps of the direct kernel,
+    the staged kernel, four single chll_lattice_pass calls per sweep and the
+    fused passes issued one by one all follow one chain bit for bit (same
+    units, counters and arithmetic), with the same control block (d, step,
+    paccept, faccept)."""
+    from chllmodel_b200.lattice import FUSED_A, FUSED_A0, FUSED_B, FUSED_F, Lattice, coupling
+
+    cp = coupling(0.6, 1.0, 0.2, 1.1)
+    out = []
+    for kind in ("fused", "direct", "staged", "passes", "fused_passes"):
+        lat = Lattice(*shape, boundary="periodic" if periodic else "open")
+        if kind not in ("passes", "fused_passes"):
+            lat.set_kernel(kind)
+        lat.init_random(seed=21)
+        lat.set_control(0.15, step=1)
+        if kind == "passes":
+            for _ in range(9):
+                for p in range(4):
+                    lat.half_sweep(cp, p, seed=4)
+        elif kind == "fused_passes":
+            seq = [FUSED_A0, FUSED_B] + [FUSED_A, FUSED_B] * 8 + [FUSED_F]
+            for p in seq:
+                lat.half_sweep(cp, p, seed=4)
+        else:
+            lat.sweep(cp, 4, seed=4)
+            lat.sweep(cp, 5, seed=4)  # a second call: flips closed in between
+        out.append((lat.download_f4(), lat.control()))
+        lat.close()
+    for state, ctl in out[1:]:
+        assert np.array_equal(out[0][0], state)
+        assert out[0][1] == ctl
