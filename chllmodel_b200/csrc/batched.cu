@@ -168,8 +168,9 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   constexpr bool FLIP_AFTER = PHASE == kFusedB;
   for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units;
        g += (uint32_t)nct * THREADS)
-    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(D.L, D.G, g, step, d, D.cp, D.key0,
-                                                         D.key1, D.replica, nacc, nflip);
+    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(D.L, D.G, g, step, d, D.cp,
+                                                         KeyPair{D.key0, D.key1}, D.replica,
+                                                         nacc, nflip);
 }
 
 template <int PHASE, int THREADS>

@@ -29,22 +29,59 @@ struct Ctr4 {
   uint32_t v[4];
 };
 
+constexpr uint32_t kPhiloxM0 = 0xD2511F53u, kPhiloxM1 = 0xCD9E8D57u;
+constexpr uint32_t kPhiloxW0 = 0x9E3779B9u, kPhiloxW1 = 0xBB67AE85u;
+
+// One Philox round with round key (ka, kb).
+__host__ __device__ __forceinline__ Ctr4 philox_round(Ctr4 c, uint32_t ka, uint32_t kb) {
+  const uint64_t p0 = (uint64_t)kPhiloxM0 * c.v[0];
+  const uint64_t p1 = (uint64_t)kPhiloxM1 * c.v[2];
+  Ctr4 n;
+  n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ ka;
+  n.v[1] = (uint32_t)p1;
+  n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ kb;
+  n.v[3] = (uint32_t)p0;
+  return n;
+}
+
 __host__ __device__ __forceinline__ Ctr4 philox4x32_10(Ctr4 c, uint32_t k0, uint32_t k1) {
-  constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;
-  constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)kM0 * c.v[0];
-    const uint64_t p1 = (uint64_t)kM1 * c.v[2];
-    Ctr4 n;
-    n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ k0;
-    n.v[1] = (uint32_t)p1;
-    n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1;
-    n.v[3] = (uint32_t)p0;
-    c = n;
-    k0 += kW0;
-    k1 += kW1;
+    c = philox_round(c, k0, k1);
+    k0 += kPhiloxW0;
+    k1 += kPhiloxW1;
   }
+  return c;
+}
+
+// The ten round keys of one key, computed once on the host and passed to a
+// kernel by value: the rounds then read them as launch constants instead of
+// bumping the key in registers.
+struct PhiloxKeys {
+  uint32_t a[10], b[10];
+};
+
+__host__ __device__ inline PhiloxKeys philox_keys(uint32_t k0, uint32_t k1) {
+  PhiloxKeys K;
+  for (int r = 0; r < 10; ++r) {
+    K.a[r] = k0 + (uint32_t)r * kPhiloxW0;
+    K.b[r] = k1 + (uint32_t)r * kPhiloxW1;
+  }
+  return K;
+}
+
+// A key as its two words; the rounds bump it in registers.
+struct KeyPair {
+  uint32_t k0, k1;
+};
+
+__host__ __device__ __forceinline__ Ctr4 philox4x32_10(Ctr4 c, const KeyPair& K) {
+  return philox4x32_10(c, K.k0, K.k1);
+}
+
+__host__ __device__ __forceinline__ Ctr4 philox4x32_10(Ctr4 c, const PhiloxKeys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) c = philox_round(c, K.a[r], K.b[r]);
   return c;
 }
 

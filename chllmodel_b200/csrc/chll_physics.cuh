@@ -159,16 +159,16 @@ __device__ __forceinline__ void site_trials(float4& n, const Nbrs& nb, float d, 
 // the previous sweep's flips {g, step-1, replica, 2+C} (words 0, 2), the
 // director trials {g, step, replica, C} (words 0,1 and 2,3), this sweep's
 // flips {g, step, replica, 2+C} (words 0, 2).
-template <int C, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
+template <int C, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
 __device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& nb0,
                                             const Nbrs& nb1, bool v0, bool v1, uint32_t g,
                                             uint32_t step, float d, const Coupling& cp,
-                                            uint32_t key0, uint32_t key1, uint32_t replica,
+                                            const KEY& key, uint32_t replica,
                                             unsigned int& nacc, unsigned int& nflip) {
   Ctr4 rb = {{0u, 0u, 0u, 0u}}, rd = {{0u, 0u, 0u, 0u}}, rf = {{0u, 0u, 0u, 0u}};
-  if (FLIP_BEFORE) rb = philox4x32_10({{g, step - 1u, replica, 2u + (uint32_t)C}}, key0, key1);
-  if (DIR) rd = philox4x32_10({{g, step, replica, (uint32_t)C}}, key0, key1);
-  if (FLIP_AFTER) rf = philox4x32_10({{g, step, replica, 2u + (uint32_t)C}}, key0, key1);
+  if (FLIP_BEFORE) rb = philox4x32_10({{g, step - 1u, replica, 2u + (uint32_t)C}}, key);
+  if (DIR) rd = philox4x32_10({{g, step, replica, (uint32_t)C}}, key);
+  if (FLIP_AFTER) rf = philox4x32_10({{g, step, replica, 2u + (uint32_t)C}}, key);
   if (v0)
     site_trials<FLIP_BEFORE, DIR, FLIP_AFTER>(n0, nb0, d, cp, u01(rb.v[0]), u01(rd.v[0]),
                                               u01(rd.v[1]), u01(rf.v[0]), nacc, nflip);

@@ -205,8 +205,8 @@ __device__ __forceinline__ unsigned int staged_unit(const TileGeom& T, const Lat
 
   const uint32_t g = q + T.Q * (k * nj + j);
   unsigned int nacc = 0, nflip = 0;
-  unit_trials<C, false, DIRECTOR, !DIRECTOR>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp, key0,
-                                             key1, replica, nacc, nflip);
+  unit_trials<C, false, DIRECTOR, !DIRECTOR>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp,
+                                             KeyPair{key0, key1}, replica, nacc, nflip);
   float4* out = L.col[C] + ((size_t)k * nj + j) * hx + h0;
   out[0] = n0;
   out[1] = n1;

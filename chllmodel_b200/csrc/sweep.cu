@@ -160,7 +160,7 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 
 template <int PHASE, bool PERIODIC>
 __global__ void __launch_bounds__(kThreads, 3)
-    fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, uint32_t key0, uint32_t key1,
+    fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, PhiloxKeys keys,
                       uint32_t replica, Control* __restrict__ ctl) {
   constexpr int C = PHASE == kFusedB ? 1 : 0;
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   unsigned int nacc = 0, nflip = 0;
   for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
        g += gridDim.x * kThreads) {
-    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, key0,
-                                                         key1, replica, nacc, nflip);
+    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
+                                                         replica, nacc, nflip);
   }
   fused_epilogue<PHASE>(ctl, nacc, nflip, step);
 }
@@ -220,8 +220,10 @@ const StagedKernel kStaged[2][4] = {
     {staged_pass_kernel<true, 0, true>, staged_pass_kernel<true, 1, true>,
      staged_pass_kernel<false, 0, true>, staged_pass_kernel<false, 1, true>}};
 
+using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*);
+
 // [periodic][phase]
-const PassKernel kFused[2][4] = {
+const FusedKernel kFused[2][4] = {
     {fused_pass_kernel<kFusedA0, false>, fused_pass_kernel<kFusedA, false>,
      fused_pass_kernel<kFusedB, false>, fused_pass_kernel<kFusedF, false>},
     {fused_pass_kernel<kFusedA0, true>, fused_pass_kernel<kFusedA, true>,
@@ -243,7 +245,8 @@ struct DeviceShape {
 std::mutex g_shape_mutex;
 DeviceShape g_shape[64];
 
-int occupancy(PassKernel k) {
+template <class KERNEL>
+int occupancy(KERNEL k) {
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, 0);
   return n > 0 ? n : 1;
@@ -331,7 +334,8 @@ void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, 
   const uint32_t need = (G.units + kThreads - 1) / kThreads;
   const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[per][phase & 3];
   const dim3 grid(need < resident ? (need ? need : 1) : resident);
-  kFused[per][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
+  kFused[per][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1),
+                                                         replica, ctl);
 }
 
 }  // namespace chll

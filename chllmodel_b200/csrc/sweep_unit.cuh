@@ -36,10 +36,10 @@ __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 // Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.
-template <int C, bool PERIODIC, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
+template <int C, bool PERIODIC, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
-                                          uint32_t key0, uint32_t key1, uint32_t replica,
+                                          const KEY& key, uint32_t replica,
                                           unsigned int& nacc, unsigned int& nflip) {
   const uint32_t hx = (uint32_t)L.hx;
   const uint32_t nj = (uint32_t)L.nj, nk = (uint32_t)L.nk, ni = (uint32_t)L.ni;
@@ -96,8 +96,8 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
   nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
 
-  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp, key0,
-                                               key1, replica, nacc, nflip);
+  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp, key,
+                                               replica, nacc, nflip);
   cen[0] = n0;
   cen[1] = n1;
 }
@@ -110,8 +110,8 @@ __device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const S
                                                    const Coupling& cp, uint32_t key0,
                                                    uint32_t key1, uint32_t replica) {
   unsigned int nacc = 0, nflip = 0;
-  unit_step<C, PERIODIC, false, DIRECTOR, !DIRECTOR>(L, G, g, step, d, cp, key0, key1, replica,
-                                                     nacc, nflip);
+  unit_step<C, PERIODIC, false, DIRECTOR, !DIRECTOR>(L, G, g, step, d, cp, KeyPair{key0, key1},
+                                                     replica, nacc, nflip);
   return DIRECTOR ? nacc : nflip;
 }
 
