@@ -51,6 +51,7 @@ namespace {
 struct ReplicaDesc {
   LatticeView L;
   SweepGeom G;
+  MomentGeom M;
   Coupling cp;
   CouplingD cd;
   uint32_t key0, key1, replica;
@@ -166,10 +167,18 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
   constexpr bool DIR = PHASE != kFusedF;
   constexpr bool FLIP_AFTER = PHASE == kFusedB;
-  for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < D.G.units;
+  // The descriptor lives in global memory, which the lattice stores could
+  // alias as far as the compiler knows: copied into locals, its fields stay
+  // in registers instead of being reloaded for every unit.  The Philox round
+  // keys are computed once per pass, not bumped per unit.
+  const LatticeView L = D.L;
+  const SweepGeom G = D.G;
+  const Coupling cp = D.cp;
+  const PhiloxKeys key = philox_keys(D.key0, D.key1);
+  const uint32_t replica = D.replica;
+  for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units;
        g += (uint32_t)nct * THREADS)
-    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(D.L, D.G, g, step, d, D.cp,
-                                                         KeyPair{D.key0, D.key1}, D.replica,
+    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, step, d, cp, key, replica,
                                                          nacc, nflip);
 }
 
@@ -194,11 +203,10 @@ __device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState*
   double m[kObsMoments];
 #pragma unroll
   for (int t = 0; t < kObsMoments; ++t) m[t] = 0.0;
-  const size_t per_colour = (size_t)D.L.hx * D.L.nj * D.L.nk;
-  const size_t total = 2 * per_colour;
-  for (size_t e = (size_t)rank * THREADS + threadIdx.x; e < total;
-       e += (size_t)nct * THREADS)
-    site_moments(D.L, D.cd, e, per_colour, m);
+  const uint64_t total = 2ull * D.M.per_colour;  // < 2^32
+  for (uint64_t e = (uint64_t)rank * THREADS + threadIdx.x; e < total;
+       e += (uint64_t)nct * THREADS)
+    site_moments<false>(D.L, D.M, D.cd, (uint32_t)e, m);
   __shared__ double s_m[THREADS / 32][kObsMoments];
 #pragma unroll
   for (int t = 0; t < kObsMoments; ++t) {
@@ -328,7 +336,7 @@ __device__ bool run_replica(const ReplicaDesc* __restrict__ descs,
 // replicas whose state together fits in L2, so each wave's sweeps run from
 // L2; CTAs move to their next wave as soon as their replica is done.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 768 / THREADS)
+__global__ void __launch_bounds__(THREADS, 512 / THREADS)
     batch_kernel(const ReplicaDesc* __restrict__ descs, ReplicaState* __restrict__ states,
                  const int* __restrict__ cta_map, int nwaves, double* __restrict__ partials,
                  int nsweeps, int measure_every, int measure_from, unsigned long long limit) {
@@ -661,6 +669,7 @@ int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
     D.L.hx = chll::padded_ni(s.ni) / 2;
     D.L.periodic = s.boundary;
     D.G = chll::make_geom(D.L);
+    D.M = chll::make_moment_geom(D.L);
     D.cp.eps = (float)s.eps;
     D.cp.K = (float)s.K;
     D.cp.g = (float)s.g;

@@ -13,8 +13,26 @@
 
 namespace chll {
 
+// Slots of one colour are < 2^31 (a lattice has < 2^32 sites), so all the
+// index arithmetic below is 32-bit.
 __device__ __forceinline__ float4 site_at(const LatticeView& L, int i, int j, int k) {
-  return colour_array(L, (i + j + k) & 1)[((size_t)k * L.nj + j) * L.hx + (i >> 1)];
+  return colour_array(L, (i + j + k) & 1)[((uint32_t)k * (uint32_t)L.nj + (uint32_t)j) *
+                                              (uint32_t)L.hx +
+                                          ((uint32_t)i >> 1)];
+}
+
+// Slot -> (row, plane) divisions of one lattice, built on the host.
+struct MomentGeom {
+  uint32_t per_colour;  // hx * nj * nk
+  FastDiv by_hx, by_nj;
+};
+
+__host__ inline MomentGeom make_moment_geom(const LatticeView& L) {
+  MomentGeom M;
+  M.per_colour = (uint32_t)L.hx * (uint32_t)L.nj * (uint32_t)L.nk;
+  M.by_hx = FastDiv((uint32_t)L.hx);
+  M.by_nj = FastDiv((uint32_t)L.nj);
+  return M;
 }
 
 // eps*(1 - dot^2) - K*dot*cross*sfac for a forward bond.
@@ -24,15 +42,19 @@ __device__ __forceinline__ double fwd_bond(double eps, double K, double dot, dou
 }
 
 // Storage slot e of the concatenated colour arrays (colour = e >= per_colour).
-__device__ __forceinline__ void site_moments(const LatticeView& L, const CouplingD& cp, size_t e,
-                                             size_t per_colour, double acc[kObsMoments]) {
+// REF_ETOT: also the reference etot() column acc[1] (measurement rows); the
+// batched moments leave it out.
+template <bool REF_ETOT>
+__device__ __forceinline__ void site_moments(const LatticeView& L, const MomentGeom& M,
+                                             const CouplingD& cp, uint32_t e,
+                                             double acc[kObsMoments]) {
   const double eps = cp.eps, K = cp.K, g = cp.g;
-  const int c = e >= per_colour;
-  const size_t t = e - (c ? per_colour : 0);
-  const size_t r = t / (size_t)L.hx;
-  const int h = (int)(t - r * L.hx);
-  const int k = (int)(r / (size_t)L.nj);
-  const int j = (int)(r - (size_t)k * L.nj);
+  const int c = e >= M.per_colour;
+  const uint32_t t = e - (c ? M.per_colour : 0u);
+  const uint32_t r = M.by_hx.div(t);
+  const int h = (int)(t - r * (uint32_t)L.hx);
+  const int k = (int)M.by_nj.div(r);
+  const int j = (int)(r - (uint32_t)k * (uint32_t)L.nj);
   const int i = 2 * h + ((c + j + k) & 1);
   if (i >= L.ni) return;
   const float4 nf = colour_array(L, c)[t];
@@ -43,7 +65,6 @@ __device__ __forceinline__ void site_moments(const LatticeView& L, const Couplin
   const float4 X = site_at(L, ip, j, k);
   const float4 Y = site_at(L, i, jp, k);
   const float4 Z = site_at(L, i, j, kp);
-  const float4 T = site_at(L, ip, jp, k);  // diagonal read of chll_mod.f90:438
 
   const double dx = nx * X.x + ny * X.y + nz * X.z;
   const double cx = ny * X.z - nz * X.y;
@@ -60,9 +81,12 @@ __device__ __forceinline__ void site_moments(const LatticeView& L, const Couplin
   const bool has_zp = L.periodic || (k + 1 < L.nk);
   acc[0] += (has_xp ? bx : 0.0) + (has_yp ? by : 0.0) + (has_zp ? bz : 0.0) - g * s;
 
-  const double dyt = nx * (double)T.x + ny * Y.y + nz * Y.z;
-  const double byt = fwd_bond(eps, K, dyt, cy, s, Y.w);
-  acc[1] += bx + byt + ((k + 1 < L.nk) ? bz : 0.0) - g * s;
+  if (REF_ETOT) {
+    const float4 T = site_at(L, ip, jp, k);  // diagonal read of chll_mod.f90:438
+    const double dyt = nx * (double)T.x + ny * Y.y + nz * Y.z;
+    const double byt = fwd_bond(eps, K, dyt, cy, s, Y.w);
+    acc[1] += bx + byt + ((k + 1 < L.nk) ? bz : 0.0) - g * s;
+  }
 
   acc[2] += s;
   acc[3] += nx * nx;

@@ -14,18 +14,18 @@ constexpr int kObsThreads = 256;
 constexpr int kObsMaxBlocks = 148 * 4;
 
 __global__ void __launch_bounds__(kObsThreads)
-    observables_kernel(LatticeView L, CouplingD cp, const Control* __restrict__ ctl,
+    observables_kernel(LatticeView L, MomentGeom M, CouplingD cp,
+                       const Control* __restrict__ ctl,
                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
                        double* __restrict__ row, long long step) {
   double acc[kObsMoments];
 #pragma unroll
   for (int m = 0; m < kObsMoments; ++m) acc[m] = 0.0;
 
-  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
-  const size_t total = 2 * per_colour;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-       e += (size_t)gridDim.x * blockDim.x)
-    site_moments(L, cp, e, per_colour, acc);
+  const uint64_t total = 2ull * M.per_colour;  // < 2^32
+  for (uint64_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += gridDim.x * blockDim.x)
+    site_moments<true>(L, M, cp, (uint32_t)e, acc);
 
   __shared__ double s_part[kObsThreads / 32][kObsMoments];
   __shared__ bool s_last;
@@ -92,8 +92,8 @@ void launch_observables(const LatticeView& L, const CouplingD& cp, const Control
   size_t blocks = (total + kObsThreads - 1) / kObsThreads;
   if (blocks > (size_t)kObsMaxBlocks) blocks = kObsMaxBlocks;
   if (blocks == 0) blocks = 1;
-  observables_kernel<<<(unsigned int)blocks, kObsThreads, 0, stream>>>(L, cp, ctl, partials,
-                                                                         ticket, row, step);
+  observables_kernel<<<(unsigned int)blocks, kObsThreads, 0, stream>>>(
+      L, make_moment_geom(L), cp, ctl, partials, ticket, row, step);
 }
 
 }  // namespace chll
