@@ -874,4 +874,108 @@ int chll_lattice_energy_grad(chll_lattice* L, const chll_coupling* c, float* gra
   return ok();
 }
 
+int chll_lattice_shell_corr(chll_lattice* L, int nshells, int wrap, double* gn, double* gs,
+                            double* counts) {
+  if (!L || !gn || !gs || !counts) return fail(CHLL_EINVAL, "shell_corr: null argument");
+  if (nshells < 1 || nshells > chll::kMaxCorrShells)
+    return fail(CHLL_EINVAL, "shell_corr: nshells must be 1..%d (got %d)", chll::kMaxCorrShells,
+                nshells);
+  const int ni = L->ni, nj = L->nj, nk = L->nk, R = nshells;
+  const double N = (double)L->nsites;
+  // d = 0 and one half-space of offsets with |d|^2 < R^2, sorted by shell;
+  // pair counts over all offsets in closed form.
+  std::vector<int4> offs;
+  std::vector<double> cnt(R, 0.0);
+  auto wrapped = [](int d, int n) { return ((d % n) + n) % n; };
+  for (int dk = -R + 1; dk < R; ++dk)
+    for (int dj = -R + 1; dj < R; ++dj)
+      for (int di = -R + 1; di < R; ++di) {
+        const int r2 = di * di + dj * dj + dk * dk;
+        if (r2 >= R * R) continue;
+        const int shell = (int)std::floor(std::sqrt((double)r2));
+        const double c = wrap ? N
+                              : (double)std::max(0, ni - std::abs(di)) *
+                                    (double)std::max(0, nj - std::abs(dj)) *
+                                    (double)std::max(0, nk - std::abs(dk));
+        cnt[shell] += c;
+        const bool origin = di == 0 && dj == 0 && dk == 0;
+        const bool half = dk > 0 || (dk == 0 && (dj > 0 || (dj == 0 && di > 0)));
+        if (!(origin || half) || c == 0.0) continue;
+        offs.push_back(wrap ? make_int4(wrapped(di, ni), wrapped(dj, nj), wrapped(dk, nk), shell)
+                            : make_int4(di, dj, dk, shell));
+      }
+  std::stable_sort(offs.begin(), offs.end(),
+                   [](const int4& a, const int4& b) { return a.w < b.w; });
+  const int blocks = chll::shell_corr_blocks((uint64_t)L->nsites);
+  const int width = 2 * R + 1;
+  CHLL_TRY(ensure_staging(L, (size_t)L->nsites * sizeof(float4)));
+  int4* d_offs = nullptr;
+  double* d_part = nullptr;
+  CHLL_CUDA_TRY(cudaMalloc(&d_offs, std::max<size_t>(1, offs.size()) * sizeof(int4)));
+  cudaError_t e = cudaMalloc(&d_part, ((size_t)blocks + 1) * width * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaFree(d_offs);
+    return fail(CHLL_ENOMEM, "shell_corr: %s", cudaGetErrorString(e));
+  }
+  std::vector<double> out(width, 0.0);
+  e = cudaMemcpyAsync(d_offs, offs.data(), offs.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                      L->stream);
+  if (e == cudaSuccess) {
+    chll::launch_unpack_f4(L->view(), (float4*)L->staging, L->stream);
+    chll::launch_shell_corr((const float4*)L->staging, ni, nj, nk, d_offs, (int)offs.size(), R,
+                            wrap != 0, d_part, blocks, d_part + (size_t)blocks * width,
+                            L->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out.data(), d_part + (size_t)blocks * width, width * sizeof(double),
+                        cudaMemcpyDeviceToHost, L->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+  cudaFree(d_offs);
+  cudaFree(d_part);
+  if (e != cudaSuccess) return fail(CHLL_ECUDA, "shell_corr: %s", cudaGetErrorString(e));
+  const double s_mean = out[2 * R] / N;
+  for (int r = 0; r < R; ++r) {
+    const double w = r == 0 ? 1.0 : 2.0;  // shells >= 1 hold d and -d
+    gn[r] = w * out[r] / cnt[r];
+    gs[r] = w * out[R + r] / cnt[r] - s_mean * s_mean;
+    counts[r] = cnt[r];
+  }
+  return ok();
+}
+
+int chll_lattice_projection(chll_lattice* L, const int* plane, long long* hist,
+                            long long* m_min, int* nbins) {
+  if (!L || !plane || !m_min || !nbins) return fail(CHLL_EINVAL, "projection: null argument");
+  const int n[3] = {L->ni, L->nj, L->nk};
+  long long lo = 0, hi = 0;
+  for (int d = 0; d < 3; ++d) {
+    const long long p = plane[d];
+    lo += p > 0 ? p : p * n[d];
+    hi += p > 0 ? p * n[d] : p;
+  }
+  const long long nb = hi - lo + 1;
+  if (nb > chll::kMaxProjectionBins)
+    return fail(CHLL_ERANGE, "projection: %lld bins exceed %d (direction too long)", nb,
+                chll::kMaxProjectionBins);
+  *m_min = lo;
+  *nbins = (int)nb;
+  if (!hist) return ok();
+  unsigned long long* d_hist = nullptr;
+  CHLL_CUDA_TRY(cudaMalloc(&d_hist, (size_t)nb * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(d_hist, 0, (size_t)nb * sizeof(unsigned long long), L->stream);
+  if (e == cudaSuccess) {
+    chll::launch_projection(L->view(), plane[0], plane[1], plane[2], lo, (int)nb, d_hist,
+                            L->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hist, d_hist, (size_t)nb * sizeof(long long), cudaMemcpyDeviceToHost,
+                        L->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+  cudaFree(d_hist);
+  if (e != cudaSuccess) return fail(CHLL_ECUDA, "projection: %s", cudaGetErrorString(e));
+  return ok();
+}
+
 }  // extern "C"

@@ -51,4 +51,17 @@ int energy_grad_max_blocks();
 void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, int colour,
                         cudaStream_t stream);
 
+// analysis.cu: shell correlations over natural-order float4 sites (offsets
+// {di, dj, dk, shell} sorted by shell; out = [sum (n.n')^2 per shell,
+// sum s s' per shell, sum s]) and the chirality histogram along an integer
+// direction p of m = p . (i+1, j+1, k+1) - m0.
+constexpr int kMaxCorrShells = 64;
+constexpr int kMaxProjectionBins = 12288;  // 48 KB of shared int bins
+int shell_corr_blocks(uint64_t nsites);
+void launch_shell_corr(const float4* site, int ni, int nj, int nk, const int4* offs, int noffs,
+                       int nshells, bool wrap, double* partials, int blocks, double* out,
+                       cudaStream_t stream);
+void launch_projection(const LatticeView& L, int px, int py, int pz, long long m0, int nbins,
+                       unsigned long long* hist, cudaStream_t stream);
+
 }  // namespace chll

@@ -256,6 +256,25 @@ int chll_batch_get_tuning(chll_batch* b, int32_t* threads, int32_t* ctas_per_sm,
 int chll_batch_autotune(chll_batch* b, int trial_sweeps, int* best_threads, int* best_ctas,
                         double* best_ms);
 
+/* ---- Analysis (the reference's notebook analyses, on the device) ---------- */
+
+/* Shell correlations of calc_n_corr / calc_s_corr (notebooks/paper_plots2.ipynb,
+ * cell 0, lines 61-112): over every ordered pair of sites at offset d with
+ * |d|^2 < nshells^2 and shell = floor(|d|), gn[shell] is the mean of
+ * (n_x . n_{x+d})^2, gs[shell] the mean of s_x s_{x+d} - <s>^2 and counts[shell]
+ * the number of pairs.  wrap = 0 keeps both sites inside the lattice (the
+ * reference); wrap = 1 takes periodic images.  Arrays of nshells doubles;
+ * nshells <= 64.  A shell with no pair gets 0/0 (NaN), as the reference. */
+int chll_lattice_shell_corr(chll_lattice* lat, int nshells, int wrap, double* gn, double* gs,
+                            double* counts);
+/* Chirality projected on an integer direction p = plane[0..2]: hist[m - m_min]
+ * is the sum of s over the sites with p . (i+1, j+1, k+1) = m (1-based
+ * coordinates, as hero_stripe.py's get_sc).  The structure factor along p,
+ * |sum_x s_x exp(-i kv p.(x+1))|^2 / N^2, is |sum_m hist[m] exp(-i kv m)|^2 / N^2.
+ * Sets *m_min and *nbins (at most 12288); hist may be NULL to ask the size. */
+int chll_lattice_projection(chll_lattice* lat, const int* plane, long long* hist,
+                            long long* m_min, int* nbins);
+
 /* ---- energy adjoint without device allocation --------------------------- */
 
 /* Same results as chll_lattice_energy_grad, for callers that cannot let a

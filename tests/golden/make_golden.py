@@ -14,6 +14,13 @@ and committed, and nothing at test time reads the reference tree.
    (the stencil fixes KK = 1.0 and has no field term).
 2. ``philox_kat.json`` -- the published Philox4x32-10 known-answer vectors
    (Salmon et al., SC'11, Random123 distribution).
+3. ``analysis_golden.npz`` -- the reference's own analysis functions run on
+   small seeded fields: calc_n_corr / calc_s_corr (notebooks/paper_plots2.ipynb,
+   cell 0) and structure_factor / get_sc
+   (notebooks/.ipynb_checkpoints/hero_stripe-checkpoint.py).  Their source is
+   read from those files and executed with the numba decorators and tqdm
+   replaced by identities (plain Python on the same arithmetic).  Directors
+   are FP32 values stored as FP64, so the FP32 device state holds them exactly.
 """
 from __future__ import annotations
 
@@ -89,8 +96,67 @@ PHILOX_KAT = [
 ]
 
 
+def _def_source(src: str, name: str) -> str:
+    """Source of top-level function `name` (without decorators) in `src`."""
+    lines = src.split("\n")
+    start = next(i for i, l in enumerate(lines) if l.startswith(f"def {name}("))
+    end = start + 1
+    while end < len(lines) and (not lines[end].strip() or lines[end][0] in " \t"):
+        end += 1
+    return "\n".join(lines[start:end]) + "\n"
+
+
+def _identity_decorator(*args, **kwargs):
+    if len(args) == 1 and callable(args[0]) and not kwargs:
+        return args[0]
+    return lambda f: f
+
+
+def _reference_analysis():
+    nb = json.load(open(os.path.join(REF, "notebooks", "paper_plots2.ipynb")))
+    cell = "".join(nb["cells"][0]["source"])
+    hero = open(os.path.join(REF, "notebooks", ".ipynb_checkpoints",
+                             "hero_stripe-checkpoint.py")).read()
+    ns = {"np": np, "jit": _identity_decorator, "njit": _identity_decorator, "prange": range,
+          "tqdm": lambda x: x}
+    for name in ("calc_n_corr", "calc_s_corr"):
+        exec(_def_source(cell, name), ns)
+    for name in ("get_sc", "structure_factor"):
+        exec(_def_source(hero, name), ns)
+    return ns
+
+
+def make_analysis_fixture(path):
+    ns = _reference_analysis()
+    rng = np.random.default_rng(20251203)
+    out = {}
+    cases = [((6, 5, 4), 3), ((7, 6, 5), 4)]
+    planes = [[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1], [1, -1, 1], [1, 1, -1]]
+    for c, (shape, nshells) in enumerate(cases):
+        ct_ = rng.uniform(-1, 1, shape).astype(np.float32)
+        st = np.sqrt(np.float32(1) - ct_ * ct_)
+        ph = rng.uniform(0, 2 * np.pi, shape).astype(np.float32)
+        nx = (st * np.cos(ph)).astype(np.float32).astype(np.float64)
+        ny = (st * np.sin(ph)).astype(np.float32).astype(np.float64)
+        nz = ct_.astype(np.float64)
+        s = np.where(rng.random(shape) < 0.45, -1, 1).astype(np.int32)
+        gn, cn = ns["calc_n_corr"](nx, ny, nz, nshells)
+        gs, cs = ns["calc_s_corr"](s, nshells)
+        out.update({f"c{c}_nx": nx, f"c{c}_ny": ny, f"c{c}_nz": nz, f"c{c}_s": s,
+                    f"c{c}_nshells": np.int64(nshells), f"c{c}_gn": gn, f"c{c}_cn": cn,
+                    f"c{c}_gs": gs, f"c{c}_cs": cs})
+        for q, p in enumerate(planes):
+            sf, kvs = ns["structure_factor"](s, 16, 0.0, 0.5, p)
+            out[f"c{c}_sf{q}"] = sf
+        out[f"c{c}_kvs"] = kvs
+    out["ncases"] = np.int64(len(cases))
+    out["planes"] = np.asarray(planes, np.int64)
+    np.savez_compressed(path, **out)
+
+
 def main():
     make_ekernel_fixture(os.path.join(HERE, "ekernel_energy.npz"))
+    make_analysis_fixture(os.path.join(HERE, "analysis_golden.npz"))
     with open(os.path.join(HERE, "philox_kat.json"), "w") as f:
         json.dump({"generator": "philox4x32-10", "vectors": PHILOX_KAT}, f, indent=1)
     print("wrote", os.listdir(HERE))
