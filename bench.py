@@ -32,6 +32,7 @@ if ROOT not in sys.path:
 L_EDGE = 480
 KT, KK, FIELD, EPS, D0, SEED = 0.3, 1.0, 0.0, 1.0, 0.1, 11
 NOUT = 100
+E2E_SWEEPS = 10000  # the 480^3 workload's run length (observables every NOUT sweeps)
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
@@ -306,7 +307,7 @@ def gpu_arm(args):
         st.close()
         sim.nx[...], sim.ny[...], sim.nz[...], sim.s[...] = x, y, z, sp
         del x, y, z, sp
-        nsw = max(args.steps, NOUT)
+        nsw = max(args.e2e_sweeps, NOUT)
         sim.run(NOUT, NOUT)  # warm-up: allocations and graph capture
         barrier()
         t0 = time.perf_counter()
@@ -464,6 +465,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-sweeps", type=int, default=E2E_SWEEPS,
+                    help="sweeps of the end-to-end ChLLSim.run (default: the workload's 10000)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-sweeps", type=int, default=2000)
