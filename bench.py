@@ -36,9 +36,9 @@ E2E_SWEEPS = 10000  # the 480^3 workload's run length (observables every NOUT sw
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
-# B) on a 256^3 launch and scaled by sites to 480^3: 386.1 MB (A) and
-# 401.3 MB (B) per launch of 16.78 M sites.
-TRAFFIC_BYTES_PER_SITE_PASS = 23.46
+# B) on a 256^3 launch and scaled by sites to 480^3: 371.0 MB (A) and
+# 369.9 MB (B) per launch of 16.78 M sites.
+TRAFFIC_BYTES_PER_SITE_PASS = 22.08
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "

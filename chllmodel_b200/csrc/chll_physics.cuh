@@ -117,48 +117,17 @@ __device__ __forceinline__ bool metropolis(float dE, float u, float inv_kT) {
   return (dE < 0.f) || (u <= __expf(__fmul_rn(-dE, inv_kT)));
 }
 
-// The trials of one site of a work unit, in chain order: the chirality flip
-// left over from the previous sweep (FLIP_BEFORE, uniform ub), the director
-// trial of this sweep (DIR, uniforms ua for the angle and uacc for the
-// acceptance), the chirality flip of this sweep (FLIP_AFTER, uniform uf).
-// The bond sums of the current director serve the flip and the director
-// trial; after an accepted trial those of the trial director serve the
-// second flip, exactly as a separate flip pass would recompute them.
-template <bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER>
-__device__ __forceinline__ void site_trials(float4& n, const Nbrs& nb, float d, const Coupling& cp,
-                                            float ub, float ua, float uacc, float uf,
-                                            unsigned int& nacc, unsigned int& nflip) {
-  BondSums o = bond_sums(n.x, n.y, n.z, nb);
-  if (FLIP_BEFORE) {
-    if (metropolis(flip_dE(o.c, n.w, cp), ub, cp.inv_kT)) {
-      n.w = -n.w;
-      ++nflip;
-    }
-  }
-  if (DIR) {
-    float mx, my, mz;
-    propose_director(n.x, n.y, n.z, d, ua, mx, my, mz);
-    const BondSums m = bond_sums(mx, my, mz, nb);
-    if (metropolis(director_dE(o, m, n.w, cp), uacc, cp.inv_kT)) {
-      n.x = mx;
-      n.y = my;
-      n.z = mz;
-      if (FLIP_AFTER) o = m;
-      ++nacc;
-    }
-  }
-  if (FLIP_AFTER) {
-    if (metropolis(flip_dE(o.c, n.w, cp), uf, cp.inv_kT)) {
-      n.w = -n.w;
-      ++nflip;
-    }
-  }
-}
-
 // Both sites of unit g of colour C (sites present: v0, v1).  Counters:
 // the previous sweep's flips {g, step-1, replica, 2+C} (words 0, 2), the
 // director trials {g, step, replica, C} (words 0,1 and 2,3), this sweep's
-// flips {g, step, replica, 2+C} (words 0, 2).
+// flips {g, step, replica, 2+C} (words 0, 2).  Trials in chain order: the
+// flip left over from the previous sweep, the director trial, this sweep's
+// flip.  The bond sums of the current director serve the flip and the
+// director trial; after an accepted trial those of the trial director serve
+// the second flip, exactly as a separate flip pass would recompute them.
+// The two sites' trials are written side by side and only their acceptance
+// depends on v0, v1, so the two independent chains interleave; a missing
+// (padding) site's arithmetic is discarded.
 template <int C, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
 __device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& nb0,
                                             const Nbrs& nb1, bool v0, bool v1, uint32_t g,
@@ -169,12 +138,44 @@ __device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& 
   if (FLIP_BEFORE) rb = philox4x32_10({{g, step - 1u, replica, 2u + (uint32_t)C}}, key);
   if (DIR) rd = philox4x32_10({{g, step, replica, (uint32_t)C}}, key);
   if (FLIP_AFTER) rf = philox4x32_10({{g, step, replica, 2u + (uint32_t)C}}, key);
-  if (v0)
-    site_trials<FLIP_BEFORE, DIR, FLIP_AFTER>(n0, nb0, d, cp, u01(rb.v[0]), u01(rd.v[0]),
-                                              u01(rd.v[1]), u01(rf.v[0]), nacc, nflip);
-  if (v1)
-    site_trials<FLIP_BEFORE, DIR, FLIP_AFTER>(n1, nb1, d, cp, u01(rb.v[2]), u01(rd.v[2]),
-                                              u01(rd.v[3]), u01(rf.v[2]), nacc, nflip);
+  BondSums o0 = bond_sums(n0.x, n0.y, n0.z, nb0);
+  BondSums o1 = bond_sums(n1.x, n1.y, n1.z, nb1);
+  if (FLIP_BEFORE) {
+    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u01(rb.v[0]), cp.inv_kT);
+    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u01(rb.v[2]), cp.inv_kT);
+    if (a0) n0.w = -n0.w;
+    if (a1) n1.w = -n1.w;
+    nflip += (unsigned int)a0 + (unsigned int)a1;
+  }
+  if (DIR) {
+    float mx0, my0, mz0, mx1, my1, mz1;
+    propose_director(n0.x, n0.y, n0.z, d, u01(rd.v[0]), mx0, my0, mz0);
+    propose_director(n1.x, n1.y, n1.z, d, u01(rd.v[2]), mx1, my1, mz1);
+    const BondSums m0 = bond_sums(mx0, my0, mz0, nb0);
+    const BondSums m1 = bond_sums(mx1, my1, mz1, nb1);
+    const bool a0 = v0 && metropolis(director_dE(o0, m0, n0.w, cp), u01(rd.v[1]), cp.inv_kT);
+    const bool a1 = v1 && metropolis(director_dE(o1, m1, n1.w, cp), u01(rd.v[3]), cp.inv_kT);
+    if (a0) {
+      n0.x = mx0;
+      n0.y = my0;
+      n0.z = mz0;
+      if (FLIP_AFTER) o0 = m0;
+    }
+    if (a1) {
+      n1.x = mx1;
+      n1.y = my1;
+      n1.z = mz1;
+      if (FLIP_AFTER) o1 = m1;
+    }
+    nacc += (unsigned int)a0 + (unsigned int)a1;
+  }
+  if (FLIP_AFTER) {
+    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u01(rf.v[0]), cp.inv_kT);
+    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u01(rf.v[2]), cp.inv_kT);
+    if (a0) n0.w = -n0.w;
+    if (a1) n1.w = -n1.w;
+    nflip += (unsigned int)a0 + (unsigned int)a1;
+  }
 }
 
 }  // namespace chll
