@@ -32,6 +32,8 @@ EXPORTS = (
     "chll_lattice_energy_grad", "chll_lattice_reserve_rows", "chll_lattice_measure",
     "chll_lattice_read_rows", "chll_energy_grad_noalloc", "chll_lattice_quench",
     "chll_lattice_set_kernel", "chll_lattice_shell_corr", "chll_lattice_projection",
+    "chll_lattice_create_slab", "chll_lattice_slab_plane", "chll_lattice_counters",
+    "chll_lattice_control_update",
     "chll_batch_create", "chll_batch_destroy", "chll_batch_set_stream", "chll_batch_sync",
     "chll_batch_init_random", "chll_batch_upload_f4", "chll_batch_download_f4", "chll_batch_run",
     "chll_batch_moments", "chll_batch_info", "chll_batch_set_tuning", "chll_batch_autotune",
@@ -143,6 +145,13 @@ def _declare(L: ct.CDLL) -> None:
     L.chll_lattice_set_kernel.restype = i32
     L.chll_lattice_quench.argtypes = [vp, P(Coupling), dbl, i32]
     L.chll_lattice_quench.restype = i32
+    L.chll_lattice_create_slab.argtypes = [i32, i32, i32, i32, i32, i32, P(vp)]
+    L.chll_lattice_slab_plane.argtypes = [vp, i32, i32, P(vp), P(i64)]
+    L.chll_lattice_counters.argtypes = [vp, P(vp)]
+    L.chll_lattice_control_update.argtypes = [vp, i32]
+    for name in ("chll_lattice_create_slab", "chll_lattice_slab_plane", "chll_lattice_counters",
+                 "chll_lattice_control_update"):
+        getattr(L, name).restype = i32
     L.chll_lattice_shell_corr.argtypes = [vp, i32, i32, vp, vp, vp]
     L.chll_lattice_shell_corr.restype = i32
     L.chll_lattice_projection.argtypes = [vp, vp, vp, P(ct.c_longlong), P(i32)]

@@ -178,8 +178,8 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   const uint32_t replica = D.replica;
   for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units;
        g += (uint32_t)nct * THREADS)
-    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, step, d, cp, key, replica,
-                                                         nacc, nflip);
+    unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, step, d, cp, key,
+                                                                   replica, nacc, nflip);
 }
 
 template <int PHASE, int THREADS>

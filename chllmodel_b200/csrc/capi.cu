@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -21,7 +22,9 @@
 
 #include "../../include/chll_mod.h"
 #include "chll_common.cuh"
+#include "moments.cuh"
 #include "sweep.cuh"
+#include "sweep_unit.cuh"
 
 using chll::Control;
 using chll::Coupling;
@@ -155,16 +158,32 @@ struct chll_lattice {
   std::vector<GraphEntry> graphs;
   uint64_t use_clock = 0;
   int kernel = chll::kSweepAuto;
+  // z-slab of a larger lattice: global planes z0 .. z0+nk-1 of nk_global,
+  // stored as planes 2 .. nk+1 of nk+3 (plane 1 and nk+2 are the halos,
+  // plane 0 keeps the storage checkerboard equal to the global one).
+  int slab = 0, z0 = 0, nk_global = 0;
+  long long ctl_sites = 0;  // sites of the whole lattice (acceptance fractions)
 
+  int store_planes() const { return slab ? nk + 3 : nk; }
+  // The lattice's own sites (a slab's interior planes).
   LatticeView view() const {
+    const size_t off = slab ? (size_t)2 * hx * nj : 0;
     LatticeView v;
-    v.col[0] = lat;
-    v.col[1] = lat + per_colour;
+    v.col[0] = lat + off;
+    v.col[1] = lat + per_colour + off;
     v.ni = ni;
     v.nj = nj;
     v.nk = nk;
     v.hx = hx;
     v.periodic = periodic;
+    return v;
+  }
+  // All stored planes (a slab with its halos).
+  LatticeView store_view() const {
+    LatticeView v = view();
+    v.col[0] = lat;
+    v.col[1] = lat + per_colour;
+    v.nk = store_planes();
     return v;
   }
 };
@@ -329,20 +348,25 @@ int set_control_impl(chll_lattice* L, double d, long long step, long long adapt_
   c.d = d;
   c.step = step;
   c.adapt_until = adapt_until;
-  c.nsites = L->nsites;
+  c.nsites = L->ctl_sites;
+  c.deferred = L->slab;
   CHLL_CUDA_TRY(cudaMemcpyAsync(L->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, L->stream));
   CHLL_CUDA_TRY(cudaStreamSynchronize(L->stream));
   return CHLL_OK;
 }
 
 int observe_impl(chll_lattice* L, const chll::CouplingD& cp, double* dev_row, long long step) {
-  chll::launch_observables(L->view(), cp, L->ctl, L->partials, &L->tickets[0], dev_row, step,
+  const LatticeView v = L->view();
+  const chll::MomentGeom M = L->slab ? chll::make_slab_moment_geom(v, L->z0, L->nk_global)
+                                     : chll::make_moment_geom(v);
+  chll::launch_observables(v, M, cp, L->ctl, L->partials, &L->tickets[0], dev_row, step,
                            L->stream);
   CHLL_CUDA_TRY(cudaGetLastError());
   return CHLL_OK;
 }
 
-int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out) {
+int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out, int slab_z0 = -1,
+                int slab_nk = 0) {
   if (!out) return fail(CHLL_EINVAL, "lattice_create: null output pointer");
   *out = nullptr;
   if (ni < 1 || nj < 1 || nk < 1)
@@ -369,7 +393,15 @@ int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out) {
   L->hx = chll::padded_ni(ni) / 2;
   L->periodic = boundary;
   L->nsites = n;
-  L->per_colour = (size_t)L->hx * nj * nk;
+  L->ctl_sites = n;
+  if (slab_z0 >= 0) {
+    L->slab = 1;
+    L->z0 = slab_z0;
+    L->nk_global = nk;
+    L->nk = slab_nk;
+    L->nsites = (long long)ni * nj * slab_nk;
+  }
+  L->per_colour = (size_t)L->hx * nj * L->store_planes();
   cudaGetDevice(&L->device);
   auto bail = [&](cudaError_t e, const char* what) {
     chll_lattice_destroy(L);
@@ -685,7 +717,9 @@ int chll_lattice_sync(chll_lattice* L) {
 int chll_lattice_init_random(chll_lattice* L, uint64_t seed, uint32_t replica) {
   if (!L) return fail(CHLL_EINVAL, "null lattice");
   CHLL_CUDA_TRY(cudaMemsetAsync(L->lat, 0, 2 * L->per_colour * sizeof(float4), L->stream));
-  chll::launch_init_random(L->view(), seed_lo(seed), seed_hi(seed), replica, L->stream);
+  // a slab draws the values of its global sites
+  chll::launch_init_random(L->view(), seed_lo(seed), seed_hi(seed), replica, L->stream,
+                           (uint64_t)L->ni * L->nj * L->z0);
   CHLL_CUDA_TRY(cudaGetLastError());
   return ok();
 }
@@ -772,6 +806,8 @@ int chll_lattice_sweep(chll_lattice* L, const chll_coupling* c, uint64_t seed, u
   if (!L || !c) return fail(CHLL_EINVAL, "sweep: null argument");
   if (nsweeps < 0) return fail(CHLL_EINVAL, "sweep: nsweeps < 0");
   if (!(c->kT >= 0.0)) return fail(CHLL_EINVAL, "sweep: kT must be >= 0");
+  if (L->slab)
+    return fail(CHLL_EINVAL, "sweep: a slab is swept pass by pass with halo exchanges between");
   CHLL_TRY(sweep_impl(L, make_coupling(*c), seed, replica, nsweeps));
   return ok();
 }
@@ -781,6 +817,16 @@ int chll_lattice_pass(chll_lattice* L, const chll_coupling* c, uint64_t seed, ui
   if (!L || !c) return fail(CHLL_EINVAL, "pass: null argument");
   if (pass < 0 || pass > 7) return fail(CHLL_EINVAL, "pass must be 0..7 (got %d)", pass);
   if (!(c->kT >= 0.0)) return fail(CHLL_EINVAL, "pass: kT must be >= 0");
+  if (L->slab) {
+    if (pass < 4) return fail(CHLL_EINVAL, "pass: a slab runs the fused passes 4..7 only");
+    const LatticeView sv = L->store_view();
+    const chll::SweepGeom G = chll::make_slab_geom(sv, 2, L->nk, L->z0 - 2);
+    chll::launch_fused_pass(sv, G, L->periodic ? chll::kBoundSlabXY : chll::kBoundOpen,
+                            make_coupling(*c), seed_lo(seed), seed_hi(seed), replica, L->ctl,
+                            pass - 4, L->stream);
+    CHLL_CUDA_TRY(cudaGetLastError());
+    return ok();
+  }
   if (pass >= 4)
     chll::launch_fused_pass(L->view(), make_coupling(*c), seed_lo(seed), seed_hi(seed), replica,
                             L->ctl, pass - 4, L->stream);
@@ -833,6 +879,7 @@ int chll_lattice_observe(chll_lattice* L, const chll_coupling* c, double* row16)
 
 int chll_lattice_quench(chll_lattice* L, const chll_coupling* c, double eta, int nsteps) {
   if (!L || !c) return fail(CHLL_EINVAL, "quench: null argument");
+  if (L->slab) return fail(CHLL_EINVAL, "quench: not available on a slab (whole lattices only)");
   if (nsteps < 0 || !(eta >= 0.0)) return fail(CHLL_EINVAL, "quench: need nsteps >= 0, eta >= 0");
   const LatticeView v = L->view();
   const chll::CouplingD cd = make_coupling_d(*c);
@@ -847,6 +894,7 @@ int chll_lattice_quench(chll_lattice* L, const chll_coupling* c, double eta, int
 int chll_lattice_energy_grad(chll_lattice* L, const chll_coupling* c, float* grad, int project,
                              double* out4) {
   if (!L || !c) return fail(CHLL_EINVAL, "energy_grad: null argument");
+  if (L->slab) return fail(CHLL_EINVAL, "energy_grad: not available on a slab (whole lattices only)");
   const size_t total = 2 * L->per_colour;
   if (grad && !L->grad) CHLL_CUDA_TRY(cudaMalloc(&L->grad, total * sizeof(float4)));
   chll::launch_energy_grad(L->view(), make_coupling_d(*c), grad ? L->grad : nullptr, project,
@@ -877,6 +925,7 @@ int chll_lattice_energy_grad(chll_lattice* L, const chll_coupling* c, float* gra
 int chll_lattice_shell_corr(chll_lattice* L, int nshells, int wrap, double* gn, double* gs,
                             double* counts) {
   if (!L || !gn || !gs || !counts) return fail(CHLL_EINVAL, "shell_corr: null argument");
+  if (L->slab) return fail(CHLL_EINVAL, "shell_corr: not available on a slab (whole lattices only)");
   if (nshells < 1 || nshells > chll::kMaxCorrShells)
     return fail(CHLL_EINVAL, "shell_corr: nshells must be 1..%d (got %d)", chll::kMaxCorrShells,
                 nshells);
@@ -947,6 +996,7 @@ int chll_lattice_shell_corr(chll_lattice* L, int nshells, int wrap, double* gn, 
 int chll_lattice_projection(chll_lattice* L, const int* plane, long long* hist,
                             long long* m_min, int* nbins) {
   if (!L || !plane || !m_min || !nbins) return fail(CHLL_EINVAL, "projection: null argument");
+  if (L->slab) return fail(CHLL_EINVAL, "projection: not available on a slab (whole lattices only)");
   const int n[3] = {L->ni, L->nj, L->nk};
   long long lo = 0, hi = 0;
   for (int d = 0; d < 3; ++d) {
@@ -975,6 +1025,49 @@ int chll_lattice_projection(chll_lattice* L, const int* plane, long long* hist,
   if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
   cudaFree(d_hist);
   if (e != cudaSuccess) return fail(CHLL_ECUDA, "projection: %s", cudaGetErrorString(e));
+  return ok();
+}
+
+int chll_lattice_create_slab(int ni, int nj, int nk, int z0, int nkl, int boundary,
+                             chll_lattice** out) {
+  if (!out) return fail(CHLL_EINVAL, "create_slab: null output pointer");
+  *out = nullptr;
+  if (z0 < 0 || nkl < 2 || (z0 & 1) || (nkl & 1) || z0 + nkl > nk)
+    return fail(CHLL_EINVAL,
+                "create_slab: need even z0 >= 0 and even nkl >= 2 with z0 + nkl <= nk "
+                "(got z0 %d, nkl %d, nk %d)",
+                z0, nkl, nk);
+  CHLL_TRY(create_impl(ni, nj, nk, boundary, out, z0, nkl));
+  return ok();
+}
+
+int chll_lattice_slab_plane(chll_lattice* L, int colour, int which, void** ptr, int64_t* bytes) {
+  if (!L || !ptr) return fail(CHLL_EINVAL, "slab_plane: null argument");
+  if (!L->slab) return fail(CHLL_EINVAL, "slab_plane: not a slab");
+  if (colour < 0 || colour > 1 || which < 0 || which > 3)
+    return fail(CHLL_EINVAL, "slab_plane: colour 0/1 and which 0..3 (got %d, %d)", colour, which);
+  // storage planes: 1 lower halo, 2 first own plane, nk+1 last own plane, nk+2 upper halo
+  const int plane = which == 0 ? 1 : (which == 1 ? 2 : (which == 2 ? L->nk + 1 : L->nk + 2));
+  const size_t per_plane = (size_t)L->hx * L->nj;
+  *ptr = L->lat + (size_t)colour * L->per_colour + (size_t)plane * per_plane;
+  if (bytes) *bytes = (int64_t)(per_plane * sizeof(float4));
+  return ok();
+}
+
+static_assert(offsetof(Control, nflip) == offsetof(Control, nacc) + sizeof(unsigned long long),
+              "the two pass counters are read as one array");
+
+int chll_lattice_counters(chll_lattice* L, void** ptr) {
+  if (!L || !ptr) return fail(CHLL_EINVAL, "counters: null argument");
+  *ptr = &L->ctl->nacc;  // {nacc, nflip}: two consecutive uint64
+  return ok();
+}
+
+int chll_lattice_control_update(chll_lattice* L, int pass) {
+  if (!L) return fail(CHLL_EINVAL, "null lattice");
+  if (pass < 4 || pass > 7) return fail(CHLL_EINVAL, "control_update: pass 4..7 (got %d)", pass);
+  chll::launch_control_update(L->ctl, pass - 4, L->stream);
+  CHLL_CUDA_TRY(cudaGetLastError());
   return ok();
 }
 

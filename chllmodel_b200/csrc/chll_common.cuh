@@ -172,6 +172,9 @@ struct Control {
   float faccept;             // accepted flip fraction of the last sweep
   long long nacc_last;       // raw counts of the last sweep
   long long nflip_last;
+  int deferred;              // nonzero: passes only count; the epilogue runs apart
+                             // (a slab, whose counts are summed over ranks first)
+  int pad;
 };
 
 // Row written by the observables kernel (FP64).  Columns 0-4 are the

@@ -75,15 +75,16 @@ __global__ void unpack_f4_kernel(LatticeView L, float4* __restrict__ dst) {
 
 // Directors uniform on the sphere (cos(theta) = 2u-1, phi = 2*pi*u', as the
 // reference drivers' init_random, scripts/pdanneal.py:5-16) and s = -1 with
-// probability 1/2 (chll/chll.py:84-90).
-__global__ void init_random_kernel(LatticeView L, uint32_t key0, uint32_t key1,
-                                   uint32_t replica) {
+// probability 1/2 (chll/chll.py:84-90).  site0: index of the view's first
+// site in the whole lattice (a z-slab draws its global sites' values).
+__global__ void init_random_kernel(LatticeView L, uint32_t key0, uint32_t key1, uint32_t replica,
+                                   uint64_t site0) {
   const size_t n = (size_t)L.ni * L.nj * L.nk;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
        e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     site_of(L, e, i, j, k);
-    Ctr4 c = {{(uint32_t)e, 0xffffffffu, replica, kStreamInit}};
+    Ctr4 c = {{(uint32_t)(e + site0), 0xffffffffu, replica, kStreamInit}};
     const Ctr4 r = philox4x32_10(c, key0, key1);
     const float ct = 2.0f * u01(r.v[0]) - 1.0f;
     const float st = sqrtf(fmaxf(0.f, 1.0f - ct * ct));
@@ -124,9 +125,9 @@ void launch_unpack_f4(const LatticeView& L, float4* xyzs, cudaStream_t stream) {
 }
 
 void launch_init_random(const LatticeView& L, uint32_t key0, uint32_t key1, uint32_t replica,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, uint64_t site0) {
   const size_t n = (size_t)L.ni * L.nj * L.nk;
-  init_random_kernel<<<grid_for(n), 256, 0, stream>>>(L, key0, key1, replica);
+  init_random_kernel<<<grid_for(n), 256, 0, stream>>>(L, key0, key1, replica, site0);
 }
 
 }  // namespace chll

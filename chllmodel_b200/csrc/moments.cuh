@@ -21,10 +21,15 @@ __device__ __forceinline__ float4 site_at(const LatticeView& L, int i, int j, in
                                           ((uint32_t)i >> 1)];
 }
 
-// Slot -> (row, plane) divisions of one lattice, built on the host.
+// Slot -> (row, plane) divisions of one lattice, built on the host.  For a
+// z-slab (zhalo = 1) the view's planes are global planes kglob0.. of a
+// lattice of nkg planes, and the plane after the view's last one is its halo:
+// the +z bond of the last plane reads it, and exists unless the global
+// lattice ends there (open boundary).
 struct MomentGeom {
   uint32_t per_colour;  // hx * nj * nk
   FastDiv by_hx, by_nj;
+  int zhalo, kglob0, nkg;
 };
 
 __host__ inline MomentGeom make_moment_geom(const LatticeView& L) {
@@ -32,6 +37,17 @@ __host__ inline MomentGeom make_moment_geom(const LatticeView& L) {
   M.per_colour = (uint32_t)L.hx * (uint32_t)L.nj * (uint32_t)L.nk;
   M.by_hx = FastDiv((uint32_t)L.hx);
   M.by_nj = FastDiv((uint32_t)L.nj);
+  M.zhalo = 0;
+  M.kglob0 = 0;
+  M.nkg = L.nk;
+  return M;
+}
+
+__host__ inline MomentGeom make_slab_moment_geom(const LatticeView& L, int kglob0, int nkg) {
+  MomentGeom M = make_moment_geom(L);
+  M.zhalo = 1;
+  M.kglob0 = kglob0;
+  M.nkg = nkg;
   return M;
 }
 
@@ -61,7 +77,7 @@ __device__ __forceinline__ void site_moments(const LatticeView& L, const MomentG
   const double nx = nf.x, ny = nf.y, nz = nf.z, s = nf.w;
   const int ip = (i + 1 == L.ni) ? 0 : i + 1;
   const int jp = (j + 1 == L.nj) ? 0 : j + 1;
-  const int kp = (k + 1 == L.nk) ? 0 : k + 1;
+  const int kp = (k + 1 == L.nk && !M.zhalo) ? 0 : k + 1;
   const float4 X = site_at(L, ip, j, k);
   const float4 Y = site_at(L, i, jp, k);
   const float4 Z = site_at(L, i, j, kp);
@@ -78,14 +94,15 @@ __device__ __forceinline__ void site_moments(const LatticeView& L, const MomentG
 
   const bool has_xp = L.periodic || (i + 1 < L.ni);
   const bool has_yp = L.periodic || (j + 1 < L.nj);
-  const bool has_zp = L.periodic || (k + 1 < L.nk);
+  const bool ref_zp = M.kglob0 + k + 1 < M.nkg;  // z is open in etot
+  const bool has_zp = L.periodic || ref_zp;
   acc[0] += (has_xp ? bx : 0.0) + (has_yp ? by : 0.0) + (has_zp ? bz : 0.0) - g * s;
 
   if (REF_ETOT) {
     const float4 T = site_at(L, ip, jp, k);  // diagonal read of chll_mod.f90:438
     const double dyt = nx * (double)T.x + ny * Y.y + nz * Y.z;
     const double byt = fwd_bond(eps, K, dyt, cy, s, Y.w);
-    acc[1] += bx + byt + ((k + 1 < L.nk) ? bz : 0.0) - g * s;
+    acc[1] += bx + byt + (ref_zp ? bz : 0.0) - g * s;
   }
 
   acc[2] += s;

@@ -85,15 +85,21 @@ __global__ void __launch_bounds__(kObsThreads)
 
 int observables_max_blocks() { return kObsMaxBlocks; }
 
-void launch_observables(const LatticeView& L, const CouplingD& cp, const Control* ctl,
-                        double* partials, unsigned int* ticket, double* row, long long step,
-                        cudaStream_t stream) {
+void launch_observables(const LatticeView& L, const MomentGeom& M, const CouplingD& cp,
+                        const Control* ctl, double* partials, unsigned int* ticket, double* row,
+                        long long step, cudaStream_t stream) {
   const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;
   size_t blocks = (total + kObsThreads - 1) / kObsThreads;
   if (blocks > (size_t)kObsMaxBlocks) blocks = kObsMaxBlocks;
   if (blocks == 0) blocks = 1;
-  observables_kernel<<<(unsigned int)blocks, kObsThreads, 0, stream>>>(
-      L, make_moment_geom(L), cp, ctl, partials, ticket, row, step);
+  observables_kernel<<<(unsigned int)blocks, kObsThreads, 0, stream>>>(L, M, cp, ctl, partials,
+                                                                        ticket, row, step);
+}
+
+void launch_observables(const LatticeView& L, const CouplingD& cp, const Control* ctl,
+                        double* partials, unsigned int* ticket, double* row, long long step,
+                        cudaStream_t stream) {
+  launch_observables(L, make_moment_geom(L), cp, ctl, partials, ticket, row, step, stream);
 }
 
 }  // namespace chll

@@ -110,6 +110,28 @@ __global__ void __launch_bounds__(kThreads, 3)
 // Control epilogue (last CTA): B closes the director count (paccept, d) and
 // advances the step; A and F close the previous sweep's flip count
 // (faccept), which B started with the colour-1 flips.
+// The control update after a fused pass, from the counts in the control
+// block: B closes the director count (paccept, d) and advances the step, A
+// and F close the previous step's flip count (faccept).
+template <int PHASE>
+__device__ __forceinline__ void fused_control_update(Control* __restrict__ ctl, long long step) {
+  const float n3 = (float)ctl->nsites;
+  if (PHASE == kFusedB) {
+    const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
+    const float pa = (float)na / n3;  // chll_mod.f90:83
+    ctl->paccept = pa;
+    ctl->nacc_last = (long long)na;
+    ctl->nacc = 0;
+    if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
+    ctl->step = step + 1;
+  } else if (PHASE == kFusedA || PHASE == kFusedF) {
+    const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
+    ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
+    ctl->nflip_last = (long long)nf;
+    ctl->nflip = 0;
+  }
+}
+
 template <int PHASE>
 __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsigned int nacc,
                                                unsigned int nflip, long long step) {
@@ -140,28 +162,14 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
   if (s_last && tid == 0) {
     __threadfence();
     ctl->done = 0;
-    const float n3 = (float)ctl->nsites;
-    if (PHASE == kFusedB) {
-      const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
-      const float pa = (float)na / n3;  // chll_mod.f90:83
-      ctl->paccept = pa;
-      ctl->nacc_last = (long long)na;
-      ctl->nacc = 0;
-      if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
-      ctl->step = step + 1;
-    } else if (PHASE == kFusedA || PHASE == kFusedF) {
-      const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
-      ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
-      ctl->nflip_last = (long long)nf;
-      ctl->nflip = 0;
-    }
+    if (!ctl->deferred) fused_control_update<PHASE>(ctl, step);
   }
 }
 
 // Two CTAs per SM: the two sites' interleaved trials want up to 128
 // registers, and measured, 2 x 256 threads run these passes faster than 3 x 256
 // at 80 registers.
-template <int PHASE, bool PERIODIC>
+template <int PHASE, int BMODE>
 __global__ void __launch_bounds__(kThreads, 2)
     fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, PhiloxKeys keys,
                       uint32_t replica, Control* __restrict__ ctl) {
@@ -169,15 +177,24 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
   constexpr bool DIR = PHASE != kFusedF;
   constexpr bool FLIP_AFTER = PHASE == kFusedB;
+  constexpr bool PXY = BMODE != kBoundOpen;
+  constexpr bool PZ = BMODE == kBoundPeriodic;
   const long long step = ctl->step;
   const float d = (float)ctl->d;
   unsigned int nacc = 0, nflip = 0;
-  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
+  for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units;
        g += gridDim.x * kThreads) {
-    unit_step<C, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
-                                                         replica, nacc, nflip);
+    unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
+                                                        replica, nacc, nflip);
   }
   fused_epilogue<PHASE>(ctl, nacc, nflip, step);
+}
+
+// The deferred control update of a fused pass (one thread), after the caller
+// has replaced the pass's count with its sum over all slabs.
+template <int PHASE>
+__global__ void control_update_kernel(Control* __restrict__ ctl) {
+  fused_control_update<PHASE>(ctl, ctl->step);
 }
 
 // Staged kernel: row tiles come into shared memory by bulk copies one tile
@@ -225,12 +242,14 @@ const StagedKernel kStaged[2][4] = {
 
 using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*);
 
-// [periodic][phase]
-const FusedKernel kFused[2][4] = {
-    {fused_pass_kernel<kFusedA0, false>, fused_pass_kernel<kFusedA, false>,
-     fused_pass_kernel<kFusedB, false>, fused_pass_kernel<kFusedF, false>},
-    {fused_pass_kernel<kFusedA0, true>, fused_pass_kernel<kFusedA, true>,
-     fused_pass_kernel<kFusedB, true>, fused_pass_kernel<kFusedF, true>}};
+// [boundary mode][phase]
+const FusedKernel kFused[3][4] = {
+    {fused_pass_kernel<kFusedA0, kBoundOpen>, fused_pass_kernel<kFusedA, kBoundOpen>,
+     fused_pass_kernel<kFusedB, kBoundOpen>, fused_pass_kernel<kFusedF, kBoundOpen>},
+    {fused_pass_kernel<kFusedA0, kBoundPeriodic>, fused_pass_kernel<kFusedA, kBoundPeriodic>,
+     fused_pass_kernel<kFusedB, kBoundPeriodic>, fused_pass_kernel<kFusedF, kBoundPeriodic>},
+    {fused_pass_kernel<kFusedA0, kBoundSlabXY>, fused_pass_kernel<kFusedA, kBoundSlabXY>,
+     fused_pass_kernel<kFusedB, kBoundSlabXY>, fused_pass_kernel<kFusedF, kBoundSlabXY>}};
 
 // Largest dynamic shared memory a staged CTA may ask for (2 stages).
 constexpr size_t kStagedSmemMax = 200 * 1024;
@@ -241,7 +260,7 @@ constexpr size_t kStagedSmemMax = 200 * 1024;
 struct DeviceShape {
   int sms = 0;
   int per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  int fused_per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  int fused_per_sm[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
   size_t staged_smem[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last size asked per kernel
   int staged_per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
@@ -268,6 +287,7 @@ DeviceShape& device_shape() {
       for (int p = 0; p < 4; ++p) {
         s.per_sm[per][p] = occupancy(kKernels[per][p]);
         s.fused_per_sm[per][p] = occupancy(kFused[per][p]);
+        if (per == 1) s.fused_per_sm[2][p] = occupancy(kFused[2][p]);
         cudaFuncSetAttribute(kStaged[per][p], cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kStagedSmemMax);
       }
@@ -329,16 +349,32 @@ void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, 
   kKernels[per][pass & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, key0, key1, replica, ctl);
 }
 
+void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, const Coupling& cp,
+                       uint32_t key0, uint32_t key1, uint32_t replica, Control* ctl, int phase,
+                       cudaStream_t stream) {
+  DeviceShape& ds = device_shape();
+  const int m = bmode < 0 ? 0 : (bmode > 2 ? 2 : bmode);
+  const uint32_t n = G.units - G.first;
+  const uint32_t need = (n + kThreads - 1) / kThreads;
+  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3];
+  const dim3 grid(need < resident ? (need ? need : 1) : resident);
+  kFused[m][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1), replica,
+                                                       ctl);
+}
+
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int phase, cudaStream_t stream) {
-  DeviceShape& ds = device_shape();
-  const int per = L.periodic ? 1 : 0;
-  const SweepGeom G = make_geom(L);
-  const uint32_t need = (G.units + kThreads - 1) / kThreads;
-  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[per][phase & 3];
-  const dim3 grid(need < resident ? (need ? need : 1) : resident);
-  kFused[per][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1),
-                                                         replica, ctl);
+  launch_fused_pass(L, make_geom(L), L.periodic ? kBoundPeriodic : kBoundOpen, cp, key0, key1,
+                    replica, ctl, phase, stream);
+}
+
+void launch_control_update(Control* ctl, int phase, cudaStream_t stream) {
+  switch (phase & 3) {
+    case kFusedA: control_update_kernel<kFusedA><<<1, 1, 0, stream>>>(ctl); break;
+    case kFusedB: control_update_kernel<kFusedB><<<1, 1, 0, stream>>>(ctl); break;
+    case kFusedF: control_update_kernel<kFusedF><<<1, 1, 0, stream>>>(ctl); break;
+    default: break;  // A0 closes no count
+  }
 }
 
 }  // namespace chll

@@ -25,6 +25,14 @@ bool staged_fits(const LatticeView& L);
 enum FusedPhase : int { kFusedA0 = 0, kFusedA = 1, kFusedB = 2, kFusedF = 3 };
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int phase, cudaStream_t stream);
+// The same on an explicit unit range and boundary mode (sweep_unit.cuh:
+// make_slab_geom, BoundaryMode), for a z-slab with halo planes.
+struct SweepGeom;
+void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, const Coupling& cp,
+                       uint32_t key0, uint32_t key1, uint32_t replica, Control* ctl, int phase,
+                       cudaStream_t stream);
+// The control update of a fused pass when the control block defers it.
+void launch_control_update(Control* ctl, int phase, cudaStream_t stream);
 
 // layout.cu: natural-order (F-order, i fastest) <-> red/black float4.
 void launch_pack_f64(const LatticeView& L, const double* nx, const double* ny, const double* nz,
@@ -34,13 +42,17 @@ void launch_unpack_f64(const LatticeView& L, double* nx, double* ny, double* nz,
 void launch_pack_f4(const LatticeView& L, const float4* xyzs, cudaStream_t stream);
 void launch_unpack_f4(const LatticeView& L, float4* xyzs, cudaStream_t stream);
 void launch_init_random(const LatticeView& L, uint32_t key0, uint32_t key1, uint32_t replica,
-                        cudaStream_t stream);
+                        cudaStream_t stream, uint64_t site0 = 0);
 
 // observables.cu: FP64 moments and the measurement row.
 int observables_max_blocks();
 void launch_observables(const LatticeView& L, const CouplingD& cp, const Control* ctl,
                         double* partials, unsigned int* ticket, double* row, long long step,
                         cudaStream_t stream);
+struct MomentGeom;
+void launch_observables(const LatticeView& L, const MomentGeom& M, const CouplingD& cp,
+                        const Control* ctl, double* partials, unsigned int* ticket, double* row,
+                        long long step, cudaStream_t stream);
 
 // adjoint.cu: energy gradient.
 void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,

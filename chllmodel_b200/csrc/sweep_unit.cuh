@@ -17,7 +17,9 @@ namespace chll {
 
 struct SweepGeom {
   uint32_t Q;      // units (4-site blocks) per row = hx/2
-  uint32_t units;  // Q * nj * nk
+  uint32_t first;  // first unit updated (0, or a slab's first interior plane)
+  uint32_t units;  // end of the units updated: Q * nj * nk for a whole lattice
+  uint32_t goff;   // added to a unit's index for its random counter (mod 2^32)
   FastDiv by_Q;    // unit -> row
   FastDiv by_nj;   // row -> plane
 };
@@ -25,18 +27,37 @@ struct SweepGeom {
 __host__ inline SweepGeom make_geom(const LatticeView& L) {
   SweepGeom G;
   G.Q = (uint32_t)(L.hx >> 1);
+  G.first = 0;
   G.units = G.Q * (uint32_t)L.nj * (uint32_t)L.nk;
+  G.goff = 0;
   G.by_Q = FastDiv(G.Q);
   G.by_nj = FastDiv((uint32_t)L.nj);
   return G;
 }
+
+// A z-slab's storage: planes p = 0..nk-1 of L hold global planes kbase + p
+// (kbase even, so storage and global checkerboards agree); the units of
+// planes [p0, p0 + np) are updated and draw the counters of their global
+// units.
+__host__ inline SweepGeom make_slab_geom(const LatticeView& L, int p0, int np, int kbase) {
+  SweepGeom G = make_geom(L);
+  const uint32_t per_plane = G.Q * (uint32_t)L.nj;
+  G.first = per_plane * (uint32_t)p0;
+  G.units = per_plane * (uint32_t)(p0 + np);
+  G.goff = per_plane * (uint32_t)kbase;  // two's complement for kbase < 0
+  return G;
+}
+
+// Boundary modes of the fused passes: open, periodic, and periodic in x and y
+// with z taken from the storage's own planes (a slab with halo planes).
+enum BoundaryMode : int { kBoundOpen = 0, kBoundPeriodic = 1, kBoundSlabXY = 2 };
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
 // Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.
-template <int C, bool PERIODIC, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica,
@@ -67,15 +88,18 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   // x neighbours of i0 and i1: xa = i0-1, xb = i0+1 = i1-1, xc = i1+1
   uint32_t xa = i0 - 1, xb = i0 + 1, xc = i1 + 1;
   bool hxa = i0 > 0, hxb = xb < ni, hxc = xc < ni;
-  if (PERIODIC) {
+  if (PXY) {
     if (!hjm) sjm = rs + (nj - 1) * hx;
     if (!hjp) sjp = rs - (nj - 1) * hx;
-    if (!hkm) skm = rs + (nk - 1) * plane;
-    if (!hkp) skp = rs - (nk - 1) * plane;
     if (!hxa) xa = ni - 1;
     if (!hxb) xb = 0;
     if (!hxc) xc = 0;
-    hjm = hjp = hkm = hkp = hxa = hxb = hxc = true;
+    hjm = hjp = hxa = hxb = hxc = true;
+  }
+  if (PZ) {
+    if (!hkm) skm = rs + (nk - 1) * plane;
+    if (!hkp) skp = rs - (nk - 1) * plane;
+    hkm = hkp = true;
   }
   const float4* orow = oth + rs;
   const float4 fa = hxa ? ld4(orow + (xa >> 1)) : zero;
@@ -96,8 +120,8 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
   nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
 
-  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g, step, d, cp, key,
-                                               replica, nacc, nflip);
+  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g + G.goff, step, d, cp,
+                                               key, replica, nacc, nflip);
   cen[0] = n0;
   cen[1] = n1;
 }
@@ -110,8 +134,9 @@ __device__ __forceinline__ unsigned int sweep_unit(const LatticeView& L, const S
                                                    const Coupling& cp, uint32_t key0,
                                                    uint32_t key1, uint32_t replica) {
   unsigned int nacc = 0, nflip = 0;
-  unit_step<C, PERIODIC, false, DIRECTOR, !DIRECTOR>(L, G, g, step, d, cp, KeyPair{key0, key1},
-                                                     replica, nacc, nflip);
+  unit_step<C, PERIODIC, PERIODIC, false, DIRECTOR, !DIRECTOR>(L, G, g, step, d, cp,
+                                                               KeyPair{key0, key1}, replica, nacc,
+                                                               nflip);
   return DIRECTOR ? nacc : nflip;
 }
 

@@ -256,6 +256,33 @@ int chll_batch_get_tuning(chll_batch* b, int32_t* threads, int32_t* ctas_per_sm,
 int chll_batch_autotune(chll_batch* b, int trial_sweeps, int* best_threads, int* best_ctas,
                         double* best_ms);
 
+/* ---- z-slabs: one lattice split over GPUs ---------------------------------- */
+
+/* The slab of global planes z0 .. z0+nkl-1 of an ni x nj x nk lattice (z0 and
+ * nkl even, z0 + nkl <= nk), with one halo plane on each side.  Its sites
+ * draw the random counters of their global positions, so slabs that exchange
+ * halos between passes follow the whole lattice's chain exactly.  A slab is
+ * swept pass by pass with chll_lattice_pass codes 4..7 only; each pass only
+ * counts accepts: the caller sums the count the pass closes over all slabs
+ * (codes 5 and 7: the flip count, 6: the director count; see
+ * chll_lattice_counters) and then calls chll_lattice_control_update.  Upload,
+ * download, random init and measurement rows act on the slab's own planes
+ * (a row's raw sums add up over slabs); the sweep graph, the adjoint, the
+ * quench and the analyses take whole lattices only. */
+int chll_lattice_create_slab(int ni, int nj, int nk, int z0, int nkl, int boundary,
+                             chll_lattice** out);
+/* Device address and byte size of one colour's plane of a slab: which = 0 lower
+ * halo (global z0-1), 1 first own plane (z0), 2 last own plane (z0+nkl-1),
+ * 3 upper halo (z0+nkl).  A plane is hx*nj float4 of one colour. */
+int chll_lattice_slab_plane(chll_lattice* lat, int colour, int which, void** ptr,
+                            int64_t* bytes);
+/* Device address of the control block's pass counters: two uint64 {director
+ * accepts, chirality flips}. */
+int chll_lattice_counters(chll_lattice* lat, void** ptr);
+/* The control update that pass `pass` (4..7) defers on a slab: 5 and 7 close
+ * the previous step's flip fraction, 6 the director fraction, d and the step. */
+int chll_lattice_control_update(chll_lattice* lat, int pass);
+
 /* ---- Analysis (the reference's notebook analyses, on the device) ---------- */
 
 /* Shell correlations of calc_n_corr / calc_s_corr (notebooks/paper_plots2.ipynb,

@@ -1,0 +1,73 @@
+"""z-slabs on one GPU: a lattice split into slabs that exchange halo planes
+between passes (LocalHalo) follows the whole lattice's chain bit for bit, and
+the slabs' measurement rows add up to the whole lattice's."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("shape,boundary,parts", [((16, 12, 16), "periodic", 2),
+                                                  ((16, 12, 16), "periodic", 4),
+                                                  ((12, 10, 12), "open", 3),
+                                                  ((9, 6, 10), "open", 2),
+                                                  ((8, 8, 6), "periodic", 3)])
+def test_slabs_follow_the_whole_lattice(shape, boundary, parts):
+    import torch
+
+    from chllmodel_b200.lattice import Lattice, coupling
+    from chllmodel_b200.slab import LocalHalo, SlabLattice, slab_observables, split_planes, \
+        sweep_slabs
+
+    ni, nj, nk = shape
+    cp = coupling(0.6, 1.0, 0.2, 1.1)
+    nsw = 7
+    whole = Lattice(*shape, boundary=boundary)
+    whole.init_random(31, 2)
+    whole.set_control(0.15, step=1)
+    whole.sweep(cp, nsw, seed=5, replica=2)
+    ref_state = whole.download_f4()
+    ref_ctl = whole.control()
+    ref_row = whole.observe(cp)
+    whole.close()
+
+    s = torch.cuda.Stream()
+    slabs = []
+    for z0, nkl in split_planes(nk, parts):
+        sl = SlabLattice(ni, nj, nk, z0, nkl, boundary=boundary)
+        sl.set_stream(s.cuda_stream)
+        sl.init_random(31, 2)
+        sl.set_control(0.15, step=1)
+        slabs.append(sl)
+    with torch.cuda.stream(s):
+        halo = LocalHalo(slabs)
+        sweep_slabs(slabs, halo, cp, 4, seed=5, replica=2)
+        sweep_slabs(slabs, halo, cp, nsw - 4, seed=5, replica=2)
+    s.synchronize()
+    state = np.concatenate([sl.download_f4() for sl in slabs], axis=0)
+    assert np.array_equal(state, ref_state)
+    for sl in slabs:
+        assert sl.control() == ref_ctl
+    obs = slab_observables([sl.observe(cp) for sl in slabs], ni * nj * nk)
+    assert obs["energy"] == pytest.approx(ref_row[5], rel=1e-12, abs=1e-9)
+    assert obs["eta"] * ni * nj * nk == ref_row[6]
+    assert obs["etot_ref_sum"] == pytest.approx(ref_row[13], rel=1e-12, abs=1e-9)
+    for sl in slabs:
+        sl.close()
+
+
+def test_slab_rejects_whole_lattice_calls():
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import coupling
+    from chllmodel_b200.slab import SlabLattice
+
+    with pytest.raises(_lib.ChllError, match="even"):
+        SlabLattice(8, 8, 8, 1, 2)
+    sl = SlabLattice(8, 8, 8, 2, 4)
+    with pytest.raises(_lib.ChllError, match="pass by pass"):
+        sl.sweep(coupling(1.0, 1.0), 1)
+    with pytest.raises(_lib.ChllError, match="fused passes"):
+        sl.half_sweep(coupling(1.0, 1.0), 0)
+    with pytest.raises(_lib.ChllError, match="slab"):
+        sl.quench(coupling(1.0, 1.0), 0.1, 1)
+    sl.close()
