@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kGradThreads)
   if (threadIdx.x < 4) {
     double v = 0.0;
     for (unsigned int b = 0; b < gridDim.x; ++b)
-      v += *((volatile double*)&partials[(size_t)b * 4 + threadIdx.x]);
+      v += __ldcg(&partials[(size_t)b * 4 + threadIdx.x]);  // L2, in block order
     out4[threadIdx.x] = v;
   }
   __syncthreads();

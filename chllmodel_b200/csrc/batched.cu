@@ -220,12 +220,20 @@ __device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState*
     partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
   }
   if (!group_barrier(st, nct, limit)) return false;
-  if (rank == 0 && threadIdx.x == 0) {
-    double tot[kObsMoments];
-    for (int t = 0; t < kObsMoments; ++t) tot[t] = 0.0;
-    for (int c = 0; c < nct; ++c)
-      for (int t = 0; t < kObsMoments; ++t)
-        tot[t] += *((volatile double*)&partials[(size_t)(D.cta_first + c) * kObsMoments + t]);
+  if (rank != 0) return true;
+  // The group's first CTA sums the partials, one moment per thread in CTA
+  // order.  L2 loads (the partials come from other SMs; the barrier's fences
+  // made them visible there) that the compiler may issue ahead of the adds.
+  __shared__ double s_tot[kObsMoments];
+  if (threadIdx.x < kObsMoments) {
+    const double* col = partials + (size_t)D.cta_first * kObsMoments + threadIdx.x;
+    double v = 0.0;
+    for (int c = 0; c < nct; ++c) v += __ldcg(col + (size_t)c * kObsMoments);
+    s_tot[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double* tot = s_tot;
     const double n = (double)D.nsites;
     const double e = tot[0] / n, eta = tot[2] / n;
     const double qxx = 1.5 * tot[3] / n - 0.5, qyy = 1.5 * tot[4] / n - 0.5,

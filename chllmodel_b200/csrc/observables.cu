@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kObsThreads)
   if (threadIdx.x < kObsMoments) {
     double v = 0.0;
     for (unsigned int b = 0; b < gridDim.x; ++b) {
-      v += *((volatile double*)&partials[(size_t)b * kObsMoments + threadIdx.x]);
+      v += __ldcg(&partials[(size_t)b * kObsMoments + threadIdx.x]);  // L2, in block order
     }
     s_tot[threadIdx.x] = v;
   }

@@ -149,7 +149,9 @@ int chll_lattice_download_f64(chll_lattice* lat, double* nx, double* ny, double*
 /* Natural-order (i fastest) float4 (nx, ny, nz, s) records, host or device. */
 int chll_lattice_upload_f4(chll_lattice* lat, const float* xyzs);
 int chll_lattice_download_f4(chll_lattice* lat, float* xyzs);
-/* Red/black storage: colour c array base (device) and its length in float4. */
+/* Red/black storage: colour c array base (device) and its length in float4.
+ * For a slab (chll_lattice_create_slab) this is the whole store of nk+3
+ * planes, halos included; its own planes start 2*hx*nj float4 in. */
 int chll_lattice_storage(chll_lattice* lat, void** colour0, void** colour1, int64_t* per_colour,
                          int32_t* hx);
 /* Device control block: d, step, adaptation limit. */
