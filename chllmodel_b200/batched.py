@@ -91,6 +91,23 @@ class Batch:
     def init_random(self):
         check(self._L.chll_batch_init_random(self._h))
 
+    def init_uniform(self, direction, spin_seed=None):
+        """Every site of every replica gets the director `direction` (normalised;
+        the reference drivers' init_aligned (1,0,0) and init_aligned2
+        (1/sqrt2, 0, 1/sqrt2), e.g. scripts/phase_diagram_large_lowT_1.0.py:18-26)
+        and a chirality of -1 or +1 with probability 1/2 each (as init_rand_s),
+        drawn from numpy's generator seeded with (spin_seed or the replica's
+        seed, replica index)."""
+        v = np.asarray(direction, np.float64)
+        v = (v / np.linalg.norm(v)).astype(np.float32)
+        for r, sp in enumerate(self.specs):
+            n = sp["ni"] * sp["nj"] * sp["nk"]
+            rng = np.random.default_rng([sp["seed"] if spin_seed is None else int(spin_seed), r])
+            f4 = np.empty((n, 4), np.float32)
+            f4[:, :3] = v
+            f4[:, 3] = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+            self.upload_f4(r, f4)
+
     def upload_f4(self, r, xyzs):
         a = np.ascontiguousarray(xyzs, dtype=np.float32)
         check(self._L.chll_batch_upload_f4(self._h, int(r), a.ctypes.data_as(ct.c_void_p)))

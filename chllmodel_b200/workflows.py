@@ -58,14 +58,21 @@ def anneal(lat: Lattice, schedule, sweeps_per_stage: int, *, K: float, g: float 
 
 
 def phase_diagram(kTs, gs, sizes, *, K=1.0, eps=1.0, nsweeps=2000, measure_every=10,
-                  measure_from=0, seed=1, autotune=True) -> list[dict]:
+                  measure_from=0, seed=1, autotune=True, init="random") -> list[dict]:
     """Every (kT, g) point as a replica of one batched launch; returns the
-    per-replica FP64 summaries (energy, eta, S, C_v, chi_c)."""
+    per-replica FP64 summaries (energy, eta, S, C_v, chi_c).  init: "random"
+    (directors uniform on the sphere), "aligned" (1,0,0), "aligned2"
+    (1/sqrt2, 0, 1/sqrt2) as the reference drivers' init_aligned /
+    init_aligned2, or any direction (x, y, z); spins are random either way."""
     from .batched import Batch, phase_grid
 
     specs = phase_grid(kTs, gs, sizes, K=K, eps=eps, seed=seed)
+    directions = {"aligned": (1.0, 0.0, 0.0), "aligned2": (1.0, 0.0, 1.0)}
     with Batch(specs) as b:
-        b.init_random()
+        if isinstance(init, str) and init == "random":
+            b.init_random()
+        else:
+            b.init_uniform(directions[init] if isinstance(init, str) else init)
         if autotune:
             b.autotune(trial_sweeps=10)
         b.run(nsweeps, measure_every, measure_from)

@@ -92,3 +92,24 @@ def test_chllsim_resume_is_exact(tmp_path):
     c.run(80, 40, nstart=c.step + 1)
     assert np.array_equal(a.nx, c.nx) and np.array_equal(a.s, c.s)
     assert a.d == c.d
+
+
+def test_uniform_start_of_a_batch():
+    """init_uniform gives every site the director (normalised) and +-1 spins;
+    an aligned start at low temperature without chiral coupling stays
+    nematically ordered, as the reference drivers' init_aligned2 runs."""
+    from chllmodel_b200.batched import Batch, replica
+    from chllmodel_b200.workflows import phase_diagram
+
+    specs = [replica(8, kT=0.5, K=1.0, seed=3, replica=0), replica(6, 4, 10, kT=0.5, K=1.0,
+                                                                    seed=4, replica=1)]
+    with Batch(specs) as b:
+        b.init_uniform((2.0, 0.0, 2.0))
+        for r in range(len(specs)):
+            st = b.download_f4(r)
+            want = np.array([np.sqrt(0.5), 0.0, np.sqrt(0.5)], np.float32)
+            assert np.array_equal(st[:, :3], np.broadcast_to(want, st[:, :3].shape))
+            assert set(np.unique(st[:, 3])) == {-1.0, 1.0}
+    res = phase_diagram([0.1], [0.0], [12], K=0.0, nsweeps=60, measure_every=10,
+                        autotune=False, init="aligned2")
+    assert res[0]["S"] > 0.9
