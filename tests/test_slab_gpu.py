@@ -71,3 +71,47 @@ def test_slab_rejects_whole_lattice_calls():
     with pytest.raises(_lib.ChllError, match="slab"):
         sl.quench(coupling(1.0, 1.0), 0.1, 1)
     sl.close()
+
+
+def test_torch_halo_with_one_nccl_rank():
+    """TorchHalo.for_slab (tensor views over the slab's device planes and
+    counters, NCCL all-reduce of the counts) with a one-rank group: one
+    periodic slab holding the whole lattice is its own neighbour and follows
+    the whole lattice's chain."""
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from chllmodel_b200.lattice import Lattice, coupling
+    from chllmodel_b200.slab import SlabLattice, TorchHalo, sweep_slabs
+
+    shape = (12, 10, 8)
+    cp = coupling(0.7, 1.0, 0.1)
+    whole = Lattice(*shape, boundary="periodic")
+    whole.init_random(9)
+    whole.set_control(0.2, step=1)
+    whole.sweep(cp, 5, seed=3)
+    ref = whole.download_f4(), whole.control()
+    whole.close()
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1,
+                            device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        sl = SlabLattice(*shape, 0, shape[2], boundary="periodic")
+        stream = torch.cuda.current_stream()
+        sl.set_stream(stream.cuda_stream)
+        sl.init_random(9)
+        sl.set_control(0.2, step=1)
+        sweep_slabs([sl], TorchHalo.for_slab(sl), cp, 5, seed=3)
+        torch.cuda.synchronize()
+        assert np.array_equal(sl.download_f4(), ref[0])
+        assert sl.control() == ref[1]
+        sl.close()
+    finally:
+        dist.destroy_process_group()
