@@ -1,6 +1,6 @@
 // Shared-memory staged half-sweep: the rows a tile of units needs are brought
-// into shared memory by bulk asynchronous copies (TMA, cp.async.bulk, no
-// multicast) one tile ahead of the compute, so DRAM latency overlaps the
+// into shared memory by bulk asynchronous copies (TMA, cp.async.bulk, each CTA
+// loading its own tile) one tile ahead of the compute, so DRAM latency overlaps the
 // Metropolis arithmetic instead of stalling it.
 //
 // Tile = R consecutive rows j0..j0+R-1 of one plane k (the last tile of a
