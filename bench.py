@@ -357,6 +357,8 @@ def gpu_arm(args):
                      "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
                      "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
+                     "limiter": "instruction issue (ncu on 256^3: ~300 instructions per site, "
+                                "issue 63-66%, DRAM 38-39%); bytes are the algorithmic 24 B/site",
                      "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
                      "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,
                      "four_half_sweep_equiv_gbs": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)
