@@ -145,6 +145,12 @@ class TorchHalo:
 
     @classmethod
     def for_slab(cls, slab: SlabLattice, group=None):
+        """The transport of `slab`, which from here on launches on the current
+        CUDA stream: torch orders its NCCL operations after that stream's
+        work, so passes and exchanges stay in order."""
+        import torch
+
+        slab.set_stream(torch.cuda.current_stream().cuda_stream)
         planes = {(c, w): _plane_tensor(slab, c, w) for c in (0, 1) for w in range(4)}
         return cls(lambda c, w: planes[(c, w)], _counter_tensor(slab),
                    slab.boundary == "periodic", group)
@@ -189,7 +195,9 @@ class TorchHalo:
 def sweep_slabs(slabs: list[SlabLattice], halo, cp, nsweeps: int, seed: int = 1,
                 replica: int = 0) -> None:
     """nsweeps fused sweeps of the slabs held here, exchanging halos through
-    `halo` (LocalHalo or TorchHalo); every slab ends with all trials done."""
+    `halo` (LocalHalo or TorchHalo); every slab ends with all trials done.
+    The slabs must launch on the stream that is current while this runs (the
+    halo copies and collectives are ordered on it)."""
     if nsweeps <= 0:
         return
     halo.exchange(0)
