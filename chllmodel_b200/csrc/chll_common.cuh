@@ -19,11 +19,19 @@ namespace chll {
 // as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies with the
 // published multipliers, the key bumped by the published Weyl increments
 // between rounds.  Counters used by this library:
-//   sweep passes : {group, step, replica, pass}   pass = 0..3 (see Pass)
-//   random init  : {site,  0xffffffff, replica, kStreamInit}
+//   sweeps      : {group, step', replica, colour}
+//   random init : {site,  0xffffffff, replica, kStreamInit}
 // where group = (i>>2) + (ceil(ni/4)) * (j + nj*k) is the index of the
 // 4-site x-block holding the site (two sites of each colour), and
-// site = i + ni*(j + nj*k) (0-based, F-order).
+// site = i + ni*(j + nj*k) (0-based, F-order).  One sweep call (words
+// v0..v3) gives the block's two sites w = 0, 1 of its colour all their
+// uniforms (UnitRandoms): director acceptance = top 24 bits of v[w],
+// director angle = the high (w = 0) or low (w = 1) 16 bits of v2, flip
+// acceptance = top 24 bits of v3 (w = 0) or the 24 bits
+// (v3 & 0xff)<<16 | (v0 & 0xff)<<8 | (v1 & 0xff) (w = 1).  step' is the step
+// for the director trials and the colour-1 flips of a step, and the next step
+// for the colour-0 flips (which the fused sweep runs at the start of the next
+// step's colour-0 pass): every pass then needs exactly one call per block.
 // ---------------------------------------------------------------------------
 struct Ctr4 {
   uint32_t v[4];
@@ -89,6 +97,25 @@ __host__ __device__ __forceinline__ Ctr4 philox4x32_10(Ctr4 c, const PhiloxKeys&
 // host oracle and the device read identical numbers.
 __host__ __device__ __forceinline__ float u01(uint32_t x) {
   return (float)(x >> 8) * 5.9604644775390625e-8f;  // 2^-24
+}
+
+// The uniforms of one block and colour from its sweep call (see above).
+struct UnitRandoms {
+  float acc[2];   // director acceptance
+  float ang[2];   // director angle (16-bit)
+  float flip[2];  // chirality-flip acceptance
+};
+
+__host__ __device__ __forceinline__ UnitRandoms unit_randoms(const Ctr4& r) {
+  UnitRandoms u;
+  u.acc[0] = u01(r.v[0]);
+  u.acc[1] = u01(r.v[1]);
+  u.ang[0] = (float)(r.v[2] >> 16) * 1.52587890625e-5f;      // 2^-16
+  u.ang[1] = (float)(r.v[2] & 0xffffu) * 1.52587890625e-5f;
+  u.flip[0] = u01(r.v[3]);
+  u.flip[1] = (float)(((r.v[3] & 0xffu) << 16) | ((r.v[0] & 0xffu) << 8) | (r.v[1] & 0xffu)) *
+              5.9604644775390625e-8f;
+  return u;
 }
 
 enum Pass : uint32_t {

@@ -19,7 +19,7 @@ struct Nbrs {
 // the reference) is exactly |nz| >= 0.999f for an FP32 nz.
 // The angle is taken as psi = 2*pi*(u - 1/2) in [-pi, pi), where the hardware
 // sine/cosine have absolute error <= 2^-21.4, and sin(phi) = -sin(psi),
-// cos(phi) = -cos(psi); u - 1/2 is exact for a 24-bit uniform.
+// cos(phi) = -cos(psi); u - 1/2 is exact for the 16-bit angle uniform.
 __device__ __forceinline__ void propose_director(float nx, float ny, float nz, float d, float u,
                                                  float& mx, float& my, float& mz) {
   float sn, cs;
@@ -117,44 +117,43 @@ __device__ __forceinline__ bool metropolis(float dE, float u, float inv_kT) {
   return (dE < 0.f) || (u <= __expf(__fmul_rn(-dE, inv_kT)));
 }
 
-// Both sites of unit g of colour C (sites present: v0, v1).  Counters:
-// the previous sweep's flips {g, step-1, replica, 2+C} (words 0, 2), the
-// director trials {g, step, replica, C} (words 0,1 and 2,3), this sweep's
-// flips {g, step, replica, 2+C} (words 0, 2).  Trials in chain order: the
-// flip left over from the previous sweep, the director trial, this sweep's
-// flip.  The bond sums of the current director serve the flip and the
-// director trial; after an accepted trial those of the trial director serve
-// the second flip, exactly as a separate flip pass would recompute them.
-// The two sites' trials are written side by side and only their acceptance
-// depends on v0, v1, so the two independent chains interleave; a missing
-// (padding) site's arithmetic is discarded.
+// Both sites of unit g of colour C (sites present: v0, v1), with the block's
+// one random call for this pass (chll_common.cuh: {g, step, replica, C}, or
+// step + 1 for a pass of colour-0 flips alone, the four half-sweep form's
+// flip pass).  Trials in chain order: the flip left over from the previous
+// sweep, the director trial, this sweep's flip.  The bond sums of the
+// current director serve the flip and the director trial; after an accepted
+// trial those of the trial director serve the second flip, exactly as a
+// separate flip pass would recompute them.  The two sites' trials are written
+// side by side and only their acceptance depends on v0, v1, so the two
+// independent chains interleave; a missing (padding) site's arithmetic is
+// discarded.
 template <int C, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
 __device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& nb0,
                                             const Nbrs& nb1, bool v0, bool v1, uint32_t g,
                                             uint32_t step, float d, const Coupling& cp,
                                             const KEY& key, uint32_t replica,
                                             unsigned int& nacc, unsigned int& nflip) {
-  Ctr4 rb = {{0u, 0u, 0u, 0u}}, rd = {{0u, 0u, 0u, 0u}}, rf = {{0u, 0u, 0u, 0u}};
-  if (FLIP_BEFORE) rb = philox4x32_10({{g, step - 1u, replica, 2u + (uint32_t)C}}, key);
-  if (DIR) rd = philox4x32_10({{g, step, replica, (uint32_t)C}}, key);
-  if (FLIP_AFTER) rf = philox4x32_10({{g, step, replica, 2u + (uint32_t)C}}, key);
+  constexpr bool kNextStep = FLIP_AFTER && !DIR && C == 0;
+  const UnitRandoms u = unit_randoms(
+      philox4x32_10({{g, kNextStep ? step + 1u : step, replica, (uint32_t)C}}, key));
   BondSums o0 = bond_sums(n0.x, n0.y, n0.z, nb0);
   BondSums o1 = bond_sums(n1.x, n1.y, n1.z, nb1);
   if (FLIP_BEFORE) {
-    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u01(rb.v[0]), cp.inv_kT);
-    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u01(rb.v[2]), cp.inv_kT);
+    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u.flip[0], cp.inv_kT);
+    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u.flip[1], cp.inv_kT);
     if (a0) n0.w = -n0.w;
     if (a1) n1.w = -n1.w;
     nflip += (unsigned int)a0 + (unsigned int)a1;
   }
   if (DIR) {
     float mx0, my0, mz0, mx1, my1, mz1;
-    propose_director(n0.x, n0.y, n0.z, d, u01(rd.v[0]), mx0, my0, mz0);
-    propose_director(n1.x, n1.y, n1.z, d, u01(rd.v[2]), mx1, my1, mz1);
+    propose_director(n0.x, n0.y, n0.z, d, u.ang[0], mx0, my0, mz0);
+    propose_director(n1.x, n1.y, n1.z, d, u.ang[1], mx1, my1, mz1);
     const BondSums m0 = bond_sums(mx0, my0, mz0, nb0);
     const BondSums m1 = bond_sums(mx1, my1, mz1, nb1);
-    const bool a0 = v0 && metropolis(director_dE(o0, m0, n0.w, cp), u01(rd.v[1]), cp.inv_kT);
-    const bool a1 = v1 && metropolis(director_dE(o1, m1, n1.w, cp), u01(rd.v[3]), cp.inv_kT);
+    const bool a0 = v0 && metropolis(director_dE(o0, m0, n0.w, cp), u.acc[0], cp.inv_kT);
+    const bool a1 = v1 && metropolis(director_dE(o1, m1, n1.w, cp), u.acc[1], cp.inv_kT);
     if (a0) {
       n0.x = mx0;
       n0.y = my0;
@@ -170,8 +169,8 @@ __device__ __forceinline__ void unit_trials(float4& n0, float4& n1, const Nbrs& 
     nacc += (unsigned int)a0 + (unsigned int)a1;
   }
   if (FLIP_AFTER) {
-    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u01(rf.v[0]), cp.inv_kT);
-    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u01(rf.v[2]), cp.inv_kT);
+    const bool a0 = v0 && metropolis(flip_dE(o0.c, n0.w, cp), u.flip[0], cp.inv_kT);
+    const bool a1 = v1 && metropolis(flip_dE(o1.c, n1.w, cp), u.flip[1], cp.inv_kT);
     if (a0) n0.w = -n0.w;
     if (a1) n1.w = -n1.w;
     nflip += (unsigned int)a0 + (unsigned int)a1;

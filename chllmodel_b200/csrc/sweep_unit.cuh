@@ -6,9 +6,9 @@
 // Unit g (row-major: g = q + Q*row, row = j + nj*k) is the two same-colour
 // sites of the 4-site x-block q of row (j,k): storage slots 2q and 2q+1 of
 // the colour-C array, lattice sites i0 = 4q + o and i1 = i0 + 2 with
-// o = (C+j+k)&1.  Both sites draw from one Philox call on the counter
-// {g, step, replica, pass}: director trials use words (0,1) and (2,3) as
-// (angle, acceptance), chirality trials words 0 and 2 as acceptance.
+// o = (C+j+k)&1.  Both sites draw all the uniforms of a pass from one
+// Philox call on the counter {g, step, replica, C} (chll_common.cuh,
+// UnitRandoms).
 #pragma once
 #include "chll_common.cuh"
 #include "chll_physics.cuh"

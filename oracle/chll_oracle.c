@@ -14,8 +14,16 @@
  *
  * Differences from the reference, all deliberate and shared with the GPU:
  *   - randoms come from Philox4x32-10 (Salmon et al., SC'11) keyed on
- *     (seed) and counted on (4-site x-block, step, replica, pass) instead of
- *     the unseeded Fortran random_number stream (chll_mod.f90:58,66-80);
+ *     (seed) and counted on (4-site x-block, step, replica, colour) instead
+ *     of the unseeded Fortran random_number stream (chll_mod.f90:58,66-80);
+ *     one call (words v0..v3) serves the block's two sites w = 0, 1 of that
+ *     colour: director acceptance = top 24 bits of v[w], director angle = the
+ *     high (w = 0) or low (w = 1) 16 bits of v2, flip acceptance = top 24
+ *     bits of v3 (w = 0) or the 24 bits (v3 & 0xff)<<16 | (v0 & 0xff)<<8 |
+ *     (v1 & 0xff) (w = 1).  The call of step t serves the director trials of
+ *     step t and the colour-1 flips of step t; the colour-0 flips of step t
+ *     use the colour-0 call of step t+1 (they run at the start of the next
+ *     step's colour-0 pass on the device);
  *   - a periodic boundary mode and a nematic coupling eps (eps = 1 and open
  *     boundaries reproduce the reference).
  *
@@ -58,6 +66,8 @@ void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]
 }
 
 static double u01(uint32_t x) { return (double)(x >> 8) * (1.0 / 16777216.0); }
+static double u24(uint32_t b24) { return (double)b24 * (1.0 / 16777216.0); }
+static double u16(uint32_t b16) { return (double)b16 * (1.0 / 65536.0); }
 
 static size_t at(const oracle_cfg* c, int i, int j, int k) {
   return (size_t)i + (size_t)c->ni * ((size_t)j + (size_t)c->nj * (size_t)k);
@@ -176,7 +186,8 @@ long long oracle_pass(const oracle_cfg* c, int pass, uint32_t step, double d, do
       for (int i = (colour + j + k) & 1; i < c->ni; i += 2) {
         const size_t x = at(c, i, j, k);
         const uint32_t group = (uint32_t)((i >> 2) + (size_t)ng * ((size_t)j + (size_t)c->nj * k));
-        const uint32_t ctr[4] = {group, step, c->replica, (uint32_t)pass};
+        const uint32_t cstep = (!director && colour == 0) ? step + 1u : step;
+        const uint32_t ctr[4] = {group, cstep, c->replica, (uint32_t)colour};
         uint32_t r[4];
         oracle_philox(ctr, key, r);
         const int w = (i & 3) >> 1;
@@ -186,13 +197,15 @@ long long oracle_pass(const oracle_cfg* c, int pass, uint32_t step, double d, do
         double mx = nnx, my = nny, mz = nnz;
         int snew = s[x];
         if (director) {
-          oracle_propose(nnx, nny, nnz, d, u01(r[2 * w]), &mx, &my, &mz);
+          oracle_propose(nnx, nny, nnz, d, u16(w ? (r[2] & 0xffffu) : (r[2] >> 16)), &mx, &my,
+                         &mz);
           enew = oracle_site_energy(c, nx, ny, nz, s, i, j, k, mx, my, mz, s[x]);
-          ua = u01(r[2 * w + 1]);
+          ua = u01(r[w]);
         } else {
           snew = -s[x];
           enew = oracle_site_energy(c, nx, ny, nz, s, i, j, k, nnx, nny, nnz, snew);
-          ua = u01(r[2 * w]);
+          ua = w ? u24(((r[3] & 0xffu) << 16) | ((r[0] & 0xffu) << 8) | (r[1] & 0xffu))
+                 : u01(r[3]);
         }
         int a = 0;
         if (enew < eold)
