@@ -36,9 +36,9 @@ E2E_SWEEPS = 10000  # the 480^3 workload's run length (observables every NOUT sw
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
-# B) on a 256^3 launch and scaled by sites to 480^3: 371.0 MB (A) and
-# 369.9 MB (B) per launch of 16.78 M sites.
-TRAFFIC_BYTES_PER_SITE_PASS = 22.08
+# B) on a 256^3 launch and scaled by sites to 480^3: 370.9 MB (A) and
+# 371.1 MB (B) per launch of 16.78 M sites.
+TRAFFIC_BYTES_PER_SITE_PASS = 22.11
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
@@ -357,8 +357,8 @@ def gpu_arm(args):
                      "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
                      "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
-                     "limiter": "instruction issue (ncu on 256^3: ~300 instructions per site, "
-                                "issue 63-66%, DRAM 38-39%); bytes are the algorithmic 24 B/site",
+                     "limiter": "instruction issue (ncu on 256^3: ~284 instructions per site, "
+                                "issue 61-63%, DRAM 39-40%); bytes are the algorithmic 24 B/site",
                      "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
                      "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,
                      "four_half_sweep_equiv_gbs": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)
