@@ -33,6 +33,10 @@ L_EDGE = 480
 KT, KK, FIELD, EPS, D0, SEED = 0.3, 1.0, 0.0, 1.0, 0.1, 11
 NOUT = 100
 E2E_SWEEPS = 10000  # the 480^3 workload's run length (observables every NOUT sweeps)
+# FP64 measurements of the batched grid every BATCH_NOUT sweeps in both arms,
+# as the reference's phase-diagram driver runs its 64^3 grid points
+# (scripts/phase_diagram.py:30, sim.run(200000, 50)).
+BATCH_NOUT = 50
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
@@ -379,9 +383,9 @@ def gpu_arm(args):
 def batched_vs_plain(args, rank, torch):
     """Phase-diagram grid: 64 replicas (kT on 8 points in 0.1-2.0 x h on 8 points
     in 0.0-3.0, K=1, edges drawn from {32, 48, 64}, seed 1 + replica) for
-    `batched_sweeps` sweeps with FP64 measurements every 10 sweeps, as one
-    persistent launch versus the same points run one after another with the
-    plain kernels (graph-captured 10-sweep chunks + a measurement each)."""
+    `batched_sweeps` sweeps with FP64 measurements every BATCH_NOUT sweeps, as
+    one persistent launch versus the same points run one after another with the
+    plain kernels (graph-captured BATCH_NOUT-sweep chunks + a measurement each)."""
     import numpy as np
 
     from chllmodel_b200.batched import Batch, phase_grid
@@ -401,7 +405,7 @@ def batched_vs_plain(args, rank, torch):
                 "trial_ms": None}
     else:
         tune = b.autotune(trial_sweeps=200)
-    b.run(nsw, measure_every=10)   # warm-up: graph capture and first launch
+    b.run(nsw, measure_every=BATCH_NOUT)   # warm-up: graph capture and first launch
     b.sync()
     b.close()
     b = Batch(specs)
@@ -412,7 +416,7 @@ def batched_vs_plain(args, rank, torch):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    b.run(nsw, measure_every=10)
+    b.run(nsw, measure_every=BATCH_NOUT)
     e1.record(stream)
     e1.synchronize()
     t_batched = e0.elapsed_time(e1) * 1e-3
@@ -429,17 +433,17 @@ def batched_vs_plain(args, rank, torch):
         lat.set_stream(stream.cuda_stream)
         lat.init_random(sp["seed"], sp["replica"])
         lat.set_control(sp["d"], step=1)
-        lat.reserve_rows(nsw // 10 + 1)
+        lat.reserve_rows(nsw // BATCH_NOUT + 1)
         cp = coupling(sp["kT"], sp["K"], sp["g"], sp["eps"])
-        lat.sweep(cp, 10, seed=sp["seed"], replica=sp["replica"])  # capture the graph
+        lat.sweep(cp, BATCH_NOUT, seed=sp["seed"], replica=sp["replica"])  # capture the graph
         lat.sync()
         lat.init_random(sp["seed"], sp["replica"])
         lat.set_control(sp["d"], step=1)
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record(stream)
-        for c in range(nsw // 10):
-            lat.sweep(cp, 10, seed=sp["seed"], replica=sp["replica"])
+        for c in range(nsw // BATCH_NOUT):
+            lat.sweep(cp, BATCH_NOUT, seed=sp["seed"], replica=sp["replica"])
             lat.measure(cp, c)
         a1.record(stream)
         a1.synchronize()
@@ -447,7 +451,7 @@ def batched_vs_plain(args, rank, torch):
         lat.close()
     total = info["total_sites"]
     return {"workload": "64 replicas, edges {32,48,64}^3, kT x h grid 8x8, K=1, "
-                        f"{nsw} sweeps, FP64 measurements every 10 sweeps",
+                        f"{nsw} sweeps, FP64 measurements every {BATCH_NOUT} sweeps",
             "replicas": len(specs), "total_sites": total, "sweeps": nsw,
             "time_to_grid_s": t_batched, "sequential_plain_s": t_plain,
             "speedup_vs_sequential_plain": t_plain / t_batched,
