@@ -31,17 +31,15 @@ __device__ __forceinline__ void propose_director(float nx, float ny, float nz, f
     y = __fadd_rn(ny, bb);
     z = nz;
   } else {
+    // u = (-ny, nx, 0)/rho and v = (-nz nx, -nz ny, rho^2)/rho: for a unit
+    // director |v| = rho |n| = rho, so one 1/rho scales both
     const float rho2 = fmaf(ny, ny, __fmul_rn(nx, nx));
     const float ru = rsqrtf(rho2);
-    const float ux = -__fmul_rn(ny, ru), uy = __fmul_rn(nx, ru);
-    float vx = -__fmul_rn(nz, nx), vy = -__fmul_rn(nz, ny), vz = rho2;
-    const float rv = rsqrtf(fmaf(vz, vz, fmaf(vy, vy, __fmul_rn(vx, vx))));
-    vx = __fmul_rn(vx, rv);
-    vy = __fmul_rn(vy, rv);
-    vz = __fmul_rn(vz, rv);
-    x = fmaf(bb, vx, fmaf(a, ux, nx));
-    y = fmaf(bb, vy, fmaf(a, uy, ny));
-    z = fmaf(bb, vz, nz);
+    const float ar = __fmul_rn(a, ru), br = __fmul_rn(bb, ru);
+    const float bnz = __fmul_rn(br, nz);
+    x = fmaf(-bnz, nx, fmaf(-ar, ny, nx));
+    y = fmaf(-bnz, ny, fmaf(ar, nx, ny));
+    z = fmaf(br, rho2, nz);
   }
   const float r = rsqrtf(fmaf(z, z, fmaf(y, y, __fmul_rn(x, x))));
   mx = __fmul_rn(x, r);
