@@ -7,8 +7,12 @@ reference's Python host class over it.  Submodules:
   chll         ChLLSim and the ftn_init/ftn_run ctypes prototypes
   lattice      device-resident lattices (handle API)
   batched      many replicas of uneven size in one persistent launch
+  workflows    anneal schedules and phase-diagram scans on the batched launch
   observables  S, C_v, chiral susceptibility from FP64 moments
+  analysis     shell correlations and structure factor of a lattice's state
   autograd     torch.autograd.Function over the energy adjoint kernel
+  distributed  replica sets sharded over ranks
+  slab         one lattice split into z-slabs with halo exchange
   build        nvcc build of the shared library
 """
 __version__ = "0.1.0"
