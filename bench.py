@@ -449,12 +449,29 @@ def batched_vs_plain(args, rank, torch):
         a1.synchronize()
         t_plain += a0.elapsed_time(a1) * 1e-3
         lat.close()
+    # The same points as the reference's phase-diagram driver runs them: one
+    # ChLLSim per point, run(nsweeps, BATCH_NOUT) through the C ABI with host
+    # arrays (scripts/phase_diagram.py:25-31), wall time of each run summed.
+    t_sim = float("nan")
+    if not args.no_plain_grid:
+        from chllmodel_b200 import chll
+
+        t_sim = 0.0
+        for sp in specs:
+            sim = chll.ChLLSim(sp["ni"], sp["nj"], sp["nk"], sp["kT"], sp["d"], sp["K"], sp["g"],
+                               0.0, seed=sp["seed"], boundary=sp["boundary"], epsilon=sp["eps"],
+                               verbose=False)
+            sim.init_random_directors(np.random.default_rng(sp["seed"]))
+            sim.init_rand_s()
+            t_sim += sim.run(nsw, BATCH_NOUT)
     total = info["total_sites"]
     return {"workload": "64 replicas, edges {32,48,64}^3, kT x h grid 8x8, K=1, "
                         f"{nsw} sweeps, FP64 measurements every {BATCH_NOUT} sweeps",
             "replicas": len(specs), "total_sites": total, "sweeps": nsw,
             "time_to_grid_s": t_batched, "sequential_plain_s": t_plain,
             "speedup_vs_sequential_plain": t_plain / t_batched,
+            "sequential_chllsim_s": t_sim,
+            "speedup_vs_sequential_chllsim": t_sim / t_batched,
             "site_updates_per_s": total * nsw / t_batched,
             "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "trial_ms")},
                            **{"waves": info_tune["waves"],
