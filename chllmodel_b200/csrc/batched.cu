@@ -676,6 +676,10 @@ int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
     D.L.nk = s.nk;
     D.L.hx = chll::padded_ni(s.ni) / 2;
     D.L.periodic = s.boundary;
+    if (!chll::unit_view_aligned(D.L)) {
+      chll_batch_destroy(B);
+      return fail(CHLL_ECUDA, "batch_create: replica %d storage is not 32-byte aligned", r);
+    }
     D.G = chll::make_geom(D.L);
     D.M = chll::make_moment_geom(D.L);
     D.cp.eps = (float)s.eps;

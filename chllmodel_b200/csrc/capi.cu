@@ -416,6 +416,10 @@ int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out, int sl
   L->stream = L->own_stream;
   if ((e = cudaMalloc(&L->lat, 2 * L->per_colour * sizeof(float4))) != cudaSuccess)
     return bail(e, "lattice allocation");
+  if (!chll::unit_view_aligned(L->store_view()) || !chll::unit_view_aligned(L->view())) {
+    chll_lattice_destroy(L);
+    return fail(CHLL_ECUDA, "lattice allocation is not 32-byte aligned");
+  }
   if ((e = cudaMalloc(&L->ctl, sizeof(Control))) != cudaSuccess) return bail(e, "control");
   const int pb = std::max(chll::observables_max_blocks() * chll::kObsMoments,
                           chll::energy_grad_max_blocks() * 4);

@@ -143,6 +143,13 @@ struct LatticeView {
 
 __host__ __device__ __forceinline__ int padded_ni(int ni) { return (ni + 3) & ~3; }
 
+// The sweep kernels move a unit (two float4 slots) with one 256-bit access,
+// which needs both colour arrays 32-byte aligned and rows of an even number
+// of slots.
+__host__ inline bool unit_view_aligned(const LatticeView& L) {
+  return (L.hx % 2) == 0 && ((uintptr_t)L.col[0] % 32) == 0 && ((uintptr_t)L.col[1] % 32) == 0;
+}
+
 // Colour array by a runtime colour, as a select rather than an indexed load
 // (an indexed access would move the whole view to local memory).
 __host__ __device__ __forceinline__ float4* colour_array(const LatticeView& L, int c) {

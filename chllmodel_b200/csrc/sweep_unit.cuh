@@ -54,6 +54,56 @@ enum BoundaryMode : int { kBoundOpen = 0, kBoundPeriodic = 1, kBoundSlabXY = 2 }
 
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 
+// One unit's two float4 slots as one 256-bit access (sm_100 ld/st .v8): a
+// warp's 32 units are then 1 KB of whole sectors per instruction instead of
+// two half-used 512-byte requests.  Unit starts are 32-byte aligned: every
+// colour array starts 32-byte aligned (unit_view_aligned) and a row holds an
+// even number of slots.
+struct UnitSlots {
+  float4 a, b;
+};
+
+// Read-only path: the other colour's units, which no thread of the pass writes.
+// Not a compiler barrier: every pass is one kernel launch or one call of a
+// non-inlined group loop (batched.cu), so these loads cannot move into a
+// pass that writes what they read.
+__device__ __forceinline__ UnitSlots ld_unit_nc(const float4* p) {
+  UnitSlots u;
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(u.a.x), "=f"(u.a.y), "=f"(u.a.z), "=f"(u.a.w), "=f"(u.b.x), "=f"(u.b.y),
+        "=f"(u.b.z), "=f"(u.b.w)
+      : "l"(p));
+  return u;
+}
+
+// Coherent path: the unit being updated (read, then written by this thread).
+__device__ __forceinline__ UnitSlots ld_unit(const float4* p) {
+  UnitSlots u;
+  asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(u.a.x), "=f"(u.a.y), "=f"(u.a.z), "=f"(u.a.w), "=f"(u.b.x), "=f"(u.b.y),
+                 "=f"(u.b.z), "=f"(u.b.w)
+               : "l"(p)
+               : "memory");
+  return u;
+}
+
+__device__ __forceinline__ void st_unit(float4* p, const float4& a, const float4& b) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a.x), "f"(a.y),
+               "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
+// Neighbour unit pair, or zeros past an open boundary.
+__device__ __forceinline__ void nbr_units(bool present, const float4* p, float4& s0, float4& s1) {
+  if (present) {
+    const UnitSlots u = ld_unit_nc(p);
+    s0 = u.a;
+    s1 = u.b;
+  } else {
+    s0 = s1 = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
 // Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.
@@ -79,8 +129,9 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   const bool v1 = i1 < ni;
   const uint32_t rs = row * hx;  // slot of the row start
   float4* cen = L.col[C] + rs + 2 * q;
-  float4 n0 = cen[0];
-  float4 n1 = cen[1];
+  const UnitSlots own = ld_unit(cen);
+  float4 n0 = own.a;
+  float4 n1 = own.b;
 
   // neighbour rows (slot offsets) and their presence
   uint32_t sjm = rs - hx, sjp = rs + hx, skm = rs - plane, skp = rs + plane;
@@ -111,19 +162,14 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   nb0.b[1] = fa;  // -x of i0
   nb1.b[0] = fc;  // +x of i1
   nb1.b[1] = fb;  // -x of i1
-  nb0.b[2] = hjp ? ld4(oth + sjp + h0) : zero;
-  nb1.b[2] = hjp ? ld4(oth + sjp + h0 + 1) : zero;
-  nb0.b[3] = hjm ? ld4(oth + sjm + h0) : zero;
-  nb1.b[3] = hjm ? ld4(oth + sjm + h0 + 1) : zero;
-  nb0.b[4] = hkp ? ld4(oth + skp + h0) : zero;
-  nb1.b[4] = hkp ? ld4(oth + skp + h0 + 1) : zero;
-  nb0.b[5] = hkm ? ld4(oth + skm + h0) : zero;
-  nb1.b[5] = hkm ? ld4(oth + skm + h0 + 1) : zero;
+  nbr_units(hjp, oth + sjp + h0, nb0.b[2], nb1.b[2]);
+  nbr_units(hjm, oth + sjm + h0, nb0.b[3], nb1.b[3]);
+  nbr_units(hkp, oth + skp + h0, nb0.b[4], nb1.b[4]);
+  nbr_units(hkm, oth + skm + h0, nb0.b[5], nb1.b[5]);
 
   unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g + G.goff, step, d, cp,
                                                key, replica, nacc, nflip);
-  cen[0] = n0;
-  cen[1] = n1;
+  st_unit(cen, n0, n1);
 }
 
 // One of the reference's four half-sweeps on unit g; returns the number of
