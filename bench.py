@@ -65,10 +65,14 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    _count = 0
+
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join("/tmp", f"chll_clocks_{os.getpid()}.csv")
+        ClockSampler._count += 1  # one file per sampler: several may be summarised late
+        self.path = os.path.join("/tmp", f"chll_clocks_{os.getpid()}_{ClockSampler._count}.csv")
+        self._summary = None
 
     def __enter__(self):
         try:
@@ -92,6 +96,11 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
+        if self._summary is None:
+            self._summary = self._read()
+        return self._summary
+
+    def _read(self):
         if self.proc is None or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
@@ -314,9 +323,10 @@ def gpu_arm(args):
         nsw = max(args.e2e_sweeps, NOUT)
         sim.run(NOUT, NOUT)  # warm-up: allocations and graph capture
         barrier()
-        t0 = time.perf_counter()
-        sim.run(nsw, NOUT)
-        dt = time.perf_counter() - t0
+        with ClockSampler(local) as e2e_clocks:
+            t0 = time.perf_counter()
+            sim.run(nsw, NOUT)
+            dt = time.perf_counter() - t0
         tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
         if dist is not None:
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -327,7 +337,8 @@ def gpu_arm(args):
                "h2d_bytes_per_step": h2d / nsw, "d2h_bytes_per_step": d2h / nsw,
                "sweeps": nsw, "api": "ChLLSim.run -> chll_run_ex (C ABI), pinned FP64 host "
                                      "arrays, upload + pack + sweeps + measurements + unpack + "
-                                     "download"}
+                                     "download",
+               "clocks": e2e_clocks.summary()}
 
     batched = None
     if not args.no_batched:

@@ -13,6 +13,7 @@
 // Coupling derivatives (FP64): dE/deps = sum(1-c^2), dE/dK = -sum(c*X*sbar),
 // dE/dh = -sum(s), together with E itself.
 #include "chll_common.cuh"
+#include "moments.cuh"
 #include "sweep.cuh"
 
 namespace chll {
@@ -22,8 +23,16 @@ namespace {
 constexpr int kGradThreads = 256;
 constexpr int kGradMaxBlocks = 148 * 4;
 
-__device__ __forceinline__ float4 site(const LatticeView& L, int i, int j, int k) {
-  return colour_array(L, (i + j + k) & 1)[((size_t)k * L.nj + j) * L.hx + (i >> 1)];
+// Slot t of colour `col` -> lattice site (i, j, k), with 32-bit divisions by
+// multiplication (a colour holds < 2^31 slots); false for a padding slot.
+__device__ __forceinline__ bool slot_site(const LatticeView& L, const MomentGeom& M, int col,
+                                          uint32_t t, int& i, int& j, int& k) {
+  const uint32_t r = M.by_hx.div(t);
+  const int h = (int)(t - r * (uint32_t)L.hx);
+  k = (int)M.by_nj.div(r);
+  j = (int)(r - (uint32_t)k * (uint32_t)L.nj);
+  i = 2 * h + ((col + j + k) & 1);
+  return i < L.ni;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -57,7 +66,8 @@ __device__ __forceinline__ void bond_grad(const float4& n, const float4& b, floa
 }
 
 __global__ void __launch_bounds__(kGradThreads)
-    energy_grad_kernel(LatticeView L, CouplingD cd, float4* __restrict__ grad_rb, int project,
+    energy_grad_kernel(LatticeView L, MomentGeom M, CouplingD cd, float4* __restrict__ grad_rb,
+                       int project,
                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
                        double* __restrict__ out4) {
   Coupling cp;  // FP32 couplings of the per-site gradient
@@ -66,19 +76,14 @@ __global__ void __launch_bounds__(kGradThreads)
   cp.g = (float)cd.g;
   cp.inv_kT = 0.f;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};  // E, dE/deps, dE/dK, dE/dh
-  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
-  const size_t total = 2 * per_colour;
+  const uint64_t total = 2 * (uint64_t)M.per_colour;
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-       e += (size_t)gridDim.x * blockDim.x) {
-    const int col = e >= per_colour;
-    const size_t t = e - (col ? per_colour : 0);
-    const size_t r = t / (size_t)L.hx;
-    const int h = (int)(t - r * L.hx);
-    const int k = (int)(r / (size_t)L.nj);
-    const int j = (int)(r - (size_t)k * L.nj);
-    const int i = 2 * h + ((col + j + k) & 1);
-    if (i >= L.ni) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const int col = e >= M.per_colour;
+    const uint32_t t = (uint32_t)e - (col ? M.per_colour : 0u);
+    int i, j, k;
+    if (!slot_site(L, M, col, t, i, j, k)) {
       if (grad_rb) grad_rb[e] = zero;
       continue;
     }
@@ -95,12 +100,12 @@ __global__ void __launch_bounds__(kGradThreads)
       if (!hkm) km = L.nk - 1;
       hip = him = hjp = hjm = hkp = hkm = true;
     }
-    const float4 bxp = hip ? site(L, ip, j, k) : zero;
-    const float4 bxm = him ? site(L, im, j, k) : zero;
-    const float4 byp = hjp ? site(L, i, jp, k) : zero;
-    const float4 bym = hjm ? site(L, i, jm, k) : zero;
-    const float4 bzp = hkp ? site(L, i, j, kp) : zero;
-    const float4 bzm = hkm ? site(L, i, j, km) : zero;
+    const float4 bxp = hip ? site_at(L, ip, j, k) : zero;
+    const float4 bxm = him ? site_at(L, im, j, k) : zero;
+    const float4 byp = hjp ? site_at(L, i, jp, k) : zero;
+    const float4 bym = hjm ? site_at(L, i, jm, k) : zero;
+    const float4 bzp = hkp ? site_at(L, i, j, kp) : zero;
+    const float4 bzm = hkm ? site_at(L, i, j, km) : zero;
 
     if (grad_rb) {
       float gx = 0.f, gy = 0.f, gz = 0.f;
@@ -179,19 +184,15 @@ __global__ void __launch_bounds__(kGradThreads)
 // with the neighbours (the other colour) held fixed, so the two colours
 // alternate like the Metropolis half-sweeps.  Chiralities are not changed.
 template <int C>
-__global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L, Coupling cp,
-                                                                   float eta) {
-  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
+__global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L, MomentGeom M,
+                                                                   Coupling cp, float eta) {
   float4* __restrict__ cen = L.col[C];
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < per_colour;
-       t += (size_t)gridDim.x * blockDim.x) {
-    const size_t r = t / (size_t)L.hx;
-    const int h = (int)(t - r * L.hx);
-    const int k = (int)(r / (size_t)L.nj);
-    const int j = (int)(r - (size_t)k * L.nj);
-    const int i = 2 * h + ((C + j + k) & 1);
-    if (i >= L.ni) continue;
+  for (uint64_t tt = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; tt < M.per_colour;
+       tt += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = (uint32_t)tt;
+    int i, j, k;
+    if (!slot_site(L, M, C, t, i, j, k)) continue;
     float4 n = cen[t];
     int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
     bool hip = ip < L.ni, him = im >= 0, hjp = jp < L.nj, hjm = jm >= 0, hkp = kp < L.nk,
@@ -206,12 +207,12 @@ __global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L
       hip = him = hjp = hjm = hkp = hkm = true;
     }
     float gx = 0.f, gy = 0.f, gz = 0.f;
-    bond_grad<0>(n, hip ? site(L, ip, j, k) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<0>(n, him ? site(L, im, j, k) : zero, +1.f, cp, gx, gy, gz);
-    bond_grad<1>(n, hjp ? site(L, i, jp, k) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<1>(n, hjm ? site(L, i, jm, k) : zero, +1.f, cp, gx, gy, gz);
-    bond_grad<2>(n, hkp ? site(L, i, j, kp) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<2>(n, hkm ? site(L, i, j, km) : zero, +1.f, cp, gx, gy, gz);
+    bond_grad<0>(n, hip ? site_at(L, ip, j, k) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<0>(n, him ? site_at(L, im, j, k) : zero, +1.f, cp, gx, gy, gz);
+    bond_grad<1>(n, hjp ? site_at(L, i, jp, k) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<1>(n, hjm ? site_at(L, i, jm, k) : zero, +1.f, cp, gx, gy, gz);
+    bond_grad<2>(n, hkp ? site_at(L, i, j, kp) : zero, -1.f, cp, gx, gy, gz);
+    bond_grad<2>(n, hkm ? site_at(L, i, j, km) : zero, +1.f, cp, gx, gy, gz);
     const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
     const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
     const float x = n.x - eta * (gx - gn * n.x);
@@ -236,14 +237,14 @@ void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, in
   cp.K = (float)cd.K;
   cp.g = (float)cd.g;
   cp.inv_kT = 0.f;
-  const size_t per_colour = (size_t)L.nk * L.nj * L.hx;
-  size_t blocks = (per_colour + kGradThreads - 1) / kGradThreads;
+  const MomentGeom M = make_moment_geom(L);
+  size_t blocks = ((size_t)M.per_colour + kGradThreads - 1) / kGradThreads;
   if (blocks > (size_t)148 * 8) blocks = 148 * 8;
   if (blocks == 0) blocks = 1;
   if (colour == 0)
-    quench_pass_kernel<0><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, cp, eta);
+    quench_pass_kernel<0><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, M, cp, eta);
   else
-    quench_pass_kernel<1><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, cp, eta);
+    quench_pass_kernel<1><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, M, cp, eta);
 }
 
 void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,
@@ -254,7 +255,7 @@ void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_
   if (blocks > (size_t)kGradMaxBlocks) blocks = kGradMaxBlocks;
   if (blocks == 0) blocks = 1;
   energy_grad_kernel<<<(unsigned int)blocks, kGradThreads, 0, stream>>>(
-      L, cp, grad_rb, project, partials, ticket, out4);
+      L, make_moment_geom(L), cp, grad_rb, project, partials, ticket, out4);
 }
 
 }  // namespace chll
