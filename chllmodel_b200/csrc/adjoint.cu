@@ -12,9 +12,12 @@
 // projected on the tangent plane, g - (g.n) n/|n|^2 (the torque direction).
 // Coupling derivatives (FP64): dE/deps = sum(1-c^2), dE/dK = -sum(c*X*sbar),
 // dE/dh = -sum(s), together with E itself.
+#include <algorithm>
+
 #include "chll_common.cuh"
 #include "moments.cuh"
 #include "sweep.cuh"
+#include "sweep_unit.cuh"
 
 namespace chll {
 
@@ -178,51 +181,44 @@ __global__ void __launch_bounds__(kGradThreads)
   if (threadIdx.x == 0) *ticket = 0;
 }
 
-// One colour of a zero-temperature gradient quench: every site of colour C
-// moves against its tangent-projected energy gradient,
-//   n <- normalise(n - eta * (I - n n^T) dE/dn),
-// with the neighbours (the other colour) held fixed, so the two colours
-// alternate like the Metropolis half-sweeps.  Chiralities are not changed.
-template <int C>
-__global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L, MomentGeom M,
+// One site of a zero-temperature gradient quench: n moves against its
+// tangent-projected energy gradient, n <- normalise(n - eta (I - n n^T) dE/dn),
+// with the neighbours nb (+x, -x, +y, -y, +z, -z) held fixed.
+__device__ __forceinline__ float4 quench_site(float4 n, const Nbrs& nb, const Coupling& cp,
+                                              float eta) {
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  bond_grad<0>(n, nb.b[0], -1.f, cp, gx, gy, gz);
+  bond_grad<0>(n, nb.b[1], +1.f, cp, gx, gy, gz);
+  bond_grad<1>(n, nb.b[2], -1.f, cp, gx, gy, gz);
+  bond_grad<1>(n, nb.b[3], +1.f, cp, gx, gy, gz);
+  bond_grad<2>(n, nb.b[4], -1.f, cp, gx, gy, gz);
+  bond_grad<2>(n, nb.b[5], +1.f, cp, gx, gy, gz);
+  const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+  const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
+  const float x = n.x - eta * (gx - gn * n.x);
+  const float y = n.y - eta * (gy - gn * n.y);
+  const float z = n.z - eta * (gz - gn * n.z);
+  const float rn = rsqrtf(x * x + y * y + z * z);
+  n.x = x * rn;
+  n.y = y * rn;
+  n.z = z * rn;
+  return n;
+}
+
+// One colour of the quench: every site of colour C moves with the other
+// colour fixed, so the two colours alternate like the Metropolis half-sweeps.
+// A thread takes the sweep's unit of two same-colour sites (gather_unit,
+// 256-bit accesses).  Chiralities are not changed.
+template <int C, bool PERIODIC>
+__global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L, SweepGeom G,
                                                                    Coupling cp, float eta) {
-  float4* __restrict__ cen = L.col[C];
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (uint64_t tt = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; tt < M.per_colour;
-       tt += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t t = (uint32_t)tt;
-    int i, j, k;
-    if (!slot_site(L, M, C, t, i, j, k)) continue;
-    float4 n = cen[t];
-    int ip = i + 1, im = i - 1, jp = j + 1, jm = j - 1, kp = k + 1, km = k - 1;
-    bool hip = ip < L.ni, him = im >= 0, hjp = jp < L.nj, hjm = jm >= 0, hkp = kp < L.nk,
-         hkm = km >= 0;
-    if (L.periodic) {
-      if (!hip) ip = 0;
-      if (!him) im = L.ni - 1;
-      if (!hjp) jp = 0;
-      if (!hjm) jm = L.nj - 1;
-      if (!hkp) kp = 0;
-      if (!hkm) km = L.nk - 1;
-      hip = him = hjp = hjm = hkp = hkm = true;
-    }
-    float gx = 0.f, gy = 0.f, gz = 0.f;
-    bond_grad<0>(n, hip ? site_at(L, ip, j, k) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<0>(n, him ? site_at(L, im, j, k) : zero, +1.f, cp, gx, gy, gz);
-    bond_grad<1>(n, hjp ? site_at(L, i, jp, k) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<1>(n, hjm ? site_at(L, i, jm, k) : zero, +1.f, cp, gx, gy, gz);
-    bond_grad<2>(n, hkp ? site_at(L, i, j, kp) : zero, -1.f, cp, gx, gy, gz);
-    bond_grad<2>(n, hkm ? site_at(L, i, j, km) : zero, +1.f, cp, gx, gy, gz);
-    const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
-    const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
-    const float x = n.x - eta * (gx - gn * n.x);
-    const float y = n.y - eta * (gy - gn * n.y);
-    const float z = n.z - eta * (gz - gn * n.z);
-    const float rn = rsqrtf(x * x + y * y + z * z);
-    n.x = x * rn;
-    n.y = y * rn;
-    n.z = z * rn;
-    cen[t] = n;
+  for (uint32_t g = blockIdx.x * kGradThreads + threadIdx.x; g < G.units;
+       g += gridDim.x * kGradThreads) {
+    UnitNbhd U;
+    gather_unit<C, PERIODIC, PERIODIC>(L, G, g, U);
+    if (U.v0) U.n0 = quench_site(U.n0, U.nb0, cp, eta);
+    if (U.v1) U.n1 = quench_site(U.n1, U.nb1, cp, eta);
+    st_unit(U.cen, U.n0, U.n1);
   }
 }
 
@@ -237,14 +233,30 @@ void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, in
   cp.K = (float)cd.K;
   cp.g = (float)cd.g;
   cp.inv_kT = 0.f;
-  const MomentGeom M = make_moment_geom(L);
-  size_t blocks = ((size_t)M.per_colour + kGradThreads - 1) / kGradThreads;
-  if (blocks > (size_t)148 * 8) blocks = 148 * 8;
+  // Resident CTAs of the quench kernel (same for every colour), per device.
+  static int resident[16] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& res = resident[dev & 15];
+  if (res == 0) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, quench_pass_kernel<0, true>,
+                                                  kGradThreads, 0);
+    res = std::max(1, sms) * std::max(1, per_sm);
+  }
+  const SweepGeom G = make_geom(L);
+  size_t blocks = ((size_t)G.units + kGradThreads - 1) / kGradThreads;
+  if (blocks > (size_t)res) blocks = (size_t)res;
   if (blocks == 0) blocks = 1;
-  if (colour == 0)
-    quench_pass_kernel<0><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, M, cp, eta);
-  else
-    quench_pass_kernel<1><<<(unsigned int)blocks, kGradThreads, 0, stream>>>(L, M, cp, eta);
+  const unsigned int nb = (unsigned int)blocks;
+  if (L.periodic) {
+    if (colour == 0) quench_pass_kernel<0, true><<<nb, kGradThreads, 0, stream>>>(L, G, cp, eta);
+    else quench_pass_kernel<1, true><<<nb, kGradThreads, 0, stream>>>(L, G, cp, eta);
+  } else {
+    if (colour == 0) quench_pass_kernel<0, false><<<nb, kGradThreads, 0, stream>>>(L, G, cp, eta);
+    else quench_pass_kernel<1, false><<<nb, kGradThreads, 0, stream>>>(L, G, cp, eta);
+  }
 }
 
 void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,

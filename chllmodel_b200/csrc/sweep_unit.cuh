@@ -104,14 +104,19 @@ __device__ __forceinline__ void nbr_units(bool present, const float4* p, float4&
   }
 }
 
-// Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
-// unit_trials (chll_physics.cuh), adding accepted director trials to nacc
-// and accepted flips to nflip.
-template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
-__device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
-                                          uint32_t step, float d, const Coupling& cp,
-                                          const KEY& key, uint32_t replica,
-                                          unsigned int& nacc, unsigned int& nflip) {
+// Unit g of colour C read from memory: its two sites (n0, n1; v0, v1 false
+// for padding slots), their six neighbours each (+x, -x, +y, -y, +z, -z;
+// zero past an open boundary) and the address of its slots.
+struct UnitNbhd {
+  float4* cen;
+  float4 n0, n1;
+  Nbrs nb0, nb1;
+  bool v0, v1;
+};
+
+template <int C, bool PXY, bool PZ>
+__device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeom& G, uint32_t g,
+                                            UnitNbhd& U) {
   const uint32_t hx = (uint32_t)L.hx;
   const uint32_t nj = (uint32_t)L.nj, nk = (uint32_t)L.nk, ni = (uint32_t)L.ni;
   const uint32_t plane = hx * nj;
@@ -125,13 +130,13 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   const uint32_t o = (C + j + k) & 1u;
   const uint32_t i0 = 4 * q + o;
   const uint32_t i1 = i0 + 2;
-  const bool v0 = i0 < ni;
-  const bool v1 = i1 < ni;
+  U.v0 = i0 < ni;
+  U.v1 = i1 < ni;
   const uint32_t rs = row * hx;  // slot of the row start
-  float4* cen = L.col[C] + rs + 2 * q;
-  const UnitSlots own = ld_unit(cen);
-  float4 n0 = own.a;
-  float4 n1 = own.b;
+  U.cen = L.col[C] + rs + 2 * q;
+  const UnitSlots own = ld_unit(U.cen);
+  U.n0 = own.a;
+  U.n1 = own.b;
 
   // neighbour rows (slot offsets) and their presence
   uint32_t sjm = rs - hx, sjp = rs + hx, skm = rs - plane, skp = rs + plane;
@@ -157,19 +162,29 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   const float4 fb = hxb ? ld4(orow + (xb >> 1)) : zero;
   const float4 fc = hxc ? ld4(orow + (xc >> 1)) : zero;
   const uint32_t h0 = 2 * q;
-  Nbrs nb0, nb1;
-  nb0.b[0] = fb;  // +x of i0
-  nb0.b[1] = fa;  // -x of i0
-  nb1.b[0] = fc;  // +x of i1
-  nb1.b[1] = fb;  // -x of i1
-  nbr_units(hjp, oth + sjp + h0, nb0.b[2], nb1.b[2]);
-  nbr_units(hjm, oth + sjm + h0, nb0.b[3], nb1.b[3]);
-  nbr_units(hkp, oth + skp + h0, nb0.b[4], nb1.b[4]);
-  nbr_units(hkm, oth + skm + h0, nb0.b[5], nb1.b[5]);
+  U.nb0.b[0] = fb;  // +x of i0
+  U.nb0.b[1] = fa;  // -x of i0
+  U.nb1.b[0] = fc;  // +x of i1
+  U.nb1.b[1] = fb;  // -x of i1
+  nbr_units(hjp, oth + sjp + h0, U.nb0.b[2], U.nb1.b[2]);
+  nbr_units(hjm, oth + sjm + h0, U.nb0.b[3], U.nb1.b[3]);
+  nbr_units(hkp, oth + skp + h0, U.nb0.b[4], U.nb1.b[4]);
+  nbr_units(hkm, oth + skm + h0, U.nb0.b[5], U.nb1.b[5]);
+}
 
-  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(n0, n1, nb0, nb1, v0, v1, g + G.goff, step, d, cp,
-                                               key, replica, nacc, nflip);
-  st_unit(cen, n0, n1);
+// Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
+// unit_trials (chll_physics.cuh), adding accepted director trials to nacc
+// and accepted flips to nflip.
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
+__device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
+                                          uint32_t step, float d, const Coupling& cp,
+                                          const KEY& key, uint32_t replica,
+                                          unsigned int& nacc, unsigned int& nflip) {
+  UnitNbhd U;
+  gather_unit<C, PXY, PZ>(L, G, g, U);
+  unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(U.n0, U.n1, U.nb0, U.nb1, U.v0, U.v1, g + G.goff,
+                                               step, d, cp, key, replica, nacc, nflip);
+  st_unit(U.cen, U.n0, U.n1);
 }
 
 // One of the reference's four half-sweeps on unit g; returns the number of

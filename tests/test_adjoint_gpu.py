@@ -90,3 +90,38 @@ def test_gradient_quench_lowers_energy():
     assert all(b <= a + 1e-6 for a, b in zip(energies, energies[1:]))
     assert energies[-1] < energies[0] - 0.1 * abs(energies[0])
     lat.close()
+
+
+@pytest.mark.parametrize("shape,periodic", [((12, 10, 8), True), ((9, 7, 5), False),
+                                            ((6, 6, 4), True)])
+def test_quench_step_matches_fp64_gradient(oracle, shape, periodic):
+    """One quench step on the device (colour 0, then colour 1 with colour 0
+    already moved) against n <- normalise(n - eta * projected FP64 gradient)
+    of the oracle, colour by colour; chiralities unchanged."""
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    eta = 0.05
+    lat = Lattice(*shape, boundary="periodic" if periodic else "open")
+    lat.init_random(seed=5)
+    cp = coupling(0.3, 1.0, 0.5, 1.2)
+    lat.set_control(0.1, step=1)
+    lat.sweep(cp, 3, seed=5)
+    nx, ny, nz, s = lat.download_f64()
+    cfg = oracle.make_cfg(*shape, periodic=periodic, K=1.0, g=0.5, eps=1.2)
+    i, j, k = np.indices(shape)
+    colour = (i + j + k) & 1
+    cur = [a.copy(order="F") for a in (nx, ny, nz)]
+    for c in (0, 1):
+        og, _ = oracle.energy_grad(cfg, cur[0], cur[1], cur[2], s, project=True)
+        new = [a - eta * og[..., m] for m, a in enumerate(cur)]
+        norm = np.sqrt(new[0] ** 2 + new[1] ** 2 + new[2] ** 2)
+        mask = colour == c
+        for m in range(3):
+            cur[m] = np.asfortranarray(np.where(mask, new[m] / norm, cur[m]))
+    lat.quench(cp, eta, 1)
+    gx, gy, gz, gs = lat.download_f64()
+    for got, want in zip((gx, gy, gz), cur):
+        # the gradient tolerance above (2e-5) times eta, plus FP32 rounding
+        np.testing.assert_allclose(got, want, rtol=0, atol=2e-6)
+    assert np.array_equal(gs, s)
+    lat.close()
