@@ -68,8 +68,95 @@ __device__ __forceinline__ void bond_grad(const float4& n, const float4& b, floa
   gz += a * b.z + w * (X * b.z + c * ez);
 }
 
+// dE/dn of one site from its six neighbours (+x, -x, +y, -y, +z, -z; zero
+// past an open boundary), optionally projected on the tangent plane.
+__device__ __forceinline__ float4 site_grad(const float4& n, const float4& bxp, const float4& bxm,
+                                            const float4& byp, const float4& bym,
+                                            const float4& bzp, const float4& bzm,
+                                            const Coupling& cp, int project) {
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  bond_grad<0>(n, bxp, -1.f, cp, gx, gy, gz);
+  bond_grad<0>(n, bxm, +1.f, cp, gx, gy, gz);
+  bond_grad<1>(n, byp, -1.f, cp, gx, gy, gz);
+  bond_grad<1>(n, bym, +1.f, cp, gx, gy, gz);
+  bond_grad<2>(n, bzp, -1.f, cp, gx, gy, gz);
+  bond_grad<2>(n, bzm, +1.f, cp, gx, gy, gz);
+  if (project) {
+    const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+    const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
+    gx -= gn * n.x;
+    gy -= gn * n.y;
+    gz -= gn * n.z;
+  }
+  return make_float4(gx, gy, gz, 0.f);
+}
+
+// FP64 sums of one site: its forward bonds (+x, +y, +z, each bond of the
+// lattice once; hx, hy, hz = present) and its field term.
+__device__ __forceinline__ void site_sums(const float4& n, const float4& bx, const float4& by,
+                                          const float4& bz, bool hx, bool hy, bool hz,
+                                          const CouplingD& cd, double acc[4]) {
+  const double nx = n.x, ny = n.y, nz = n.z, s = n.w;
+  const float4 fw[3] = {bx, by, bz};
+  const bool hf[3] = {hx, hy, hz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (!hf[a]) continue;
+    const float4 b = fw[a];
+    const double c = nx * b.x + ny * b.y + nz * b.z;
+    const double X = (a == 0) ? ny * b.z - nz * b.y
+                   : (a == 1) ? nz * b.x - nx * b.z
+                              : nx * b.y - ny * b.x;
+    const double sbar = 0.5 * (s + (double)b.w);
+    const double nem = 1.0 - c * c;
+    const double chi = -c * X * sbar;
+    acc[0] += cd.eps * nem + cd.K * chi;
+    acc[1] += nem;
+    acc[2] += chi;
+  }
+  acc[0] -= cd.g * s;
+  acc[3] -= s;
+}
+
+// Block sums of the four FP64 accumulators into partials; the last block to
+// finish (ticket) adds the partials in block order into out4.
+__device__ __forceinline__ void finish_sums(const double acc[4], double* __restrict__ partials,
+                                            unsigned int* __restrict__ ticket,
+                                            double* __restrict__ out4) {
+  __shared__ double s_part[kGradThreads / 32][4];
+  __shared__ bool s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const double v = warp_sum(acc[m]);
+    if (lane == 0) s_part[warp][m] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int w = 0; w < kGradThreads / 32; ++w) v += s_part[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * 4 + threadIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (unsigned int b = 0; b < gridDim.x; ++b)
+      v += __ldcg(&partials[(size_t)b * 4 + threadIdx.x]);  // L2, in block order
+    out4[threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *ticket = 0;
+}
+
+// One slot per thread: any alignment of the colour arrays (caller-provided
+// arrays of chll_energy_grad_noalloc).
 __global__ void __launch_bounds__(kGradThreads)
-    energy_grad_kernel(LatticeView L, MomentGeom M, CouplingD cd, float4* __restrict__ grad_rb,
+    energy_grad_site_kernel(LatticeView L, MomentGeom M, CouplingD cd, float4* __restrict__ grad_rb,
                        int project,
                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
                        double* __restrict__ out4) {
@@ -110,75 +197,58 @@ __global__ void __launch_bounds__(kGradThreads)
     const float4 bzp = hkp ? site_at(L, i, j, kp) : zero;
     const float4 bzm = hkm ? site_at(L, i, j, km) : zero;
 
-    if (grad_rb) {
-      float gx = 0.f, gy = 0.f, gz = 0.f;
-      bond_grad<0>(n, bxp, -1.f, cp, gx, gy, gz);
-      bond_grad<0>(n, bxm, +1.f, cp, gx, gy, gz);
-      bond_grad<1>(n, byp, -1.f, cp, gx, gy, gz);
-      bond_grad<1>(n, bym, +1.f, cp, gx, gy, gz);
-      bond_grad<2>(n, bzp, -1.f, cp, gx, gy, gz);
-      bond_grad<2>(n, bzm, +1.f, cp, gx, gy, gz);
-      if (project) {
-        const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
-        const float gn = (gx * n.x + gy * n.y + gz * n.z) / nn;
-        gx -= gn * n.x;
-        gy -= gn * n.y;
-        gz -= gn * n.z;
-      }
-      grad_rb[e] = make_float4(gx, gy, gz, 0.f);
-    }
-
-    // FP64 forward-bond sums (each bond once).
-    const double nx = n.x, ny = n.y, nz = n.z, s = n.w;
-    const float4* fw[3] = {&bxp, &byp, &bzp};
-    const bool hf[3] = {hip, hjp, hkp};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (!hf[a]) continue;
-      const float4 b = *fw[a];
-      const double c = nx * b.x + ny * b.y + nz * b.z;
-      const double X = (a == 0) ? ny * b.z - nz * b.y
-                     : (a == 1) ? nz * b.x - nx * b.z
-                                : nx * b.y - ny * b.x;
-      const double sbar = 0.5 * (s + (double)b.w);
-      const double nem = 1.0 - c * c;
-      const double chi = -c * X * sbar;
-      acc[0] += cd.eps * nem + cd.K * chi;
-      acc[1] += nem;
-      acc[2] += chi;
-    }
-    acc[0] -= cd.g * s;
-    acc[3] -= s;
+    if (grad_rb) grad_rb[e] = site_grad(n, bxp, bxm, byp, bym, bzp, bzm, cp, project);
+    site_sums(n, bxp, byp, bzp, hip, hjp, hkp, cd, acc);
   }
 
-  __shared__ double s_part[kGradThreads / 32][4];
-  __shared__ bool s_last;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    const double v = warp_sum(acc[m]);
-    if (lane == 0) s_part[warp][m] = v;
+  finish_sums(acc, partials, ticket, out4);
+}
+
+// Two sites per thread on the sweep's unit gather (256-bit accesses): colour
+// 0's units, then colour 1's.  Needs 32-byte aligned colour and gradient
+// arrays (unit_view_aligned).
+template <int C, bool PERIODIC>
+__device__ __forceinline__ void grad_units(const LatticeView& L, const SweepGeom& G,
+                                           const Coupling& cp, const CouplingD& cd,
+                                           float4* __restrict__ grad_c, int project,
+                                           double acc[4]) {
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint32_t g = blockIdx.x * kGradThreads + threadIdx.x; g < G.units;
+       g += gridDim.x * kGradThreads) {
+    UnitNbhd U;
+    gather_unit<C, PERIODIC, PERIODIC>(L, G, g, U);
+    float4 g0 = zero, g1 = zero;
+    if (U.v0) {
+      if (grad_c)
+        g0 = site_grad(U.n0, U.nb0.b[0], U.nb0.b[1], U.nb0.b[2], U.nb0.b[3], U.nb0.b[4],
+                       U.nb0.b[5], cp, project);
+      site_sums(U.n0, U.nb0.b[0], U.nb0.b[2], U.nb0.b[4], U.fx0, U.fy, U.fz, cd, acc);
+    }
+    if (U.v1) {
+      if (grad_c)
+        g1 = site_grad(U.n1, U.nb1.b[0], U.nb1.b[1], U.nb1.b[2], U.nb1.b[3], U.nb1.b[4],
+                       U.nb1.b[5], cp, project);
+      site_sums(U.n1, U.nb1.b[0], U.nb1.b[2], U.nb1.b[4], U.fx1, U.fy, U.fz, cd, acc);
+    }
+    if (grad_c) st_unit(grad_c + (U.cen - L.col[C]), g0, g1);
   }
-  __syncthreads();
-  if (threadIdx.x < 4) {
-    double v = 0.0;
-    for (int w = 0; w < kGradThreads / 32; ++w) v += s_part[w][threadIdx.x];
-    partials[(size_t)blockIdx.x * 4 + threadIdx.x] = v;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (threadIdx.x < 4) {
-    double v = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b)
-      v += __ldcg(&partials[(size_t)b * 4 + threadIdx.x]);  // L2, in block order
-    out4[threadIdx.x] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *ticket = 0;
+}
+
+template <bool PERIODIC>
+__global__ void __launch_bounds__(kGradThreads)
+    energy_grad_unit_kernel(LatticeView L, SweepGeom G, CouplingD cd,
+                            float4* __restrict__ grad_rb, uint32_t per_colour, int project,
+                            double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                            double* __restrict__ out4) {
+  Coupling cp;  // FP32 couplings of the per-site gradient
+  cp.eps = (float)cd.eps;
+  cp.K = (float)cd.K;
+  cp.g = (float)cd.g;
+  cp.inv_kT = 0.f;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};  // E, dE/deps, dE/dK, dE/dh
+  grad_units<0, PERIODIC>(L, G, cp, cd, grad_rb, project, acc);
+  grad_units<1, PERIODIC>(L, G, cp, cd, grad_rb ? grad_rb + per_colour : nullptr, project, acc);
+  finish_sums(acc, partials, ticket, out4);
 }
 
 // One site of a zero-temperature gradient quench: n moves against its
@@ -222,6 +292,22 @@ __global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L
   }
 }
 
+// CTAs of `kernel` (kGradThreads threads) resident on the current device, one
+// wave of a grid-stride launch; cached per device ordinal.
+template <class Kernel>
+int resident_ctas(Kernel kernel, int cache[16]) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& res = cache[dev & 15];
+  if (res == 0) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kGradThreads, 0);
+    res = std::max(1, sms) * std::max(1, per_sm);
+  }
+  return res;
+}
+
 }  // namespace
 
 int energy_grad_max_blocks() { return kGradMaxBlocks; }
@@ -233,18 +319,8 @@ void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, in
   cp.K = (float)cd.K;
   cp.g = (float)cd.g;
   cp.inv_kT = 0.f;
-  // Resident CTAs of the quench kernel (same for every colour), per device.
   static int resident[16] = {0};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  int& res = resident[dev & 15];
-  if (res == 0) {
-    int sms = 0, per_sm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, quench_pass_kernel<0, true>,
-                                                  kGradThreads, 0);
-    res = std::max(1, sms) * std::max(1, per_sm);
-  }
+  const int res = resident_ctas(quench_pass_kernel<0, true>, resident);
   const SweepGeom G = make_geom(L);
   size_t blocks = ((size_t)G.units + kGradThreads - 1) / kGradThreads;
   if (blocks > (size_t)res) blocks = (size_t)res;
@@ -263,11 +339,26 @@ void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_
                         double* partials, unsigned int* ticket, double* out4,
                         cudaStream_t stream) {
   const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;
-  size_t blocks = (total + kGradThreads - 1) / kGradThreads;
-  if (blocks > (size_t)kGradMaxBlocks) blocks = kGradMaxBlocks;
+  const bool units = unit_view_aligned(L) && ((uintptr_t)grad_rb % 32) == 0;
+  static int resident[16] = {0};
+  const int res = units ? resident_ctas(energy_grad_unit_kernel<true>, resident) : kGradMaxBlocks;
+  size_t blocks = ((units ? total / 4 : total) + kGradThreads - 1) / kGradThreads;
+  if (blocks > (size_t)std::min(res, kGradMaxBlocks)) blocks = std::min(res, kGradMaxBlocks);
   if (blocks == 0) blocks = 1;
-  energy_grad_kernel<<<(unsigned int)blocks, kGradThreads, 0, stream>>>(
-      L, make_moment_geom(L), cp, grad_rb, project, partials, ticket, out4);
+  const unsigned int nb = (unsigned int)blocks;
+  if (units) {
+    const SweepGeom G = make_geom(L);
+    const uint32_t pc = (uint32_t)(total / 2);
+    if (L.periodic)
+      energy_grad_unit_kernel<true><<<nb, kGradThreads, 0, stream>>>(L, G, cp, grad_rb, pc, project,
+                                                                     partials, ticket, out4);
+    else
+      energy_grad_unit_kernel<false><<<nb, kGradThreads, 0, stream>>>(
+          L, G, cp, grad_rb, pc, project, partials, ticket, out4);
+  } else {
+    energy_grad_site_kernel<<<nb, kGradThreads, 0, stream>>>(L, make_moment_geom(L), cp, grad_rb,
+                                                             project, partials, ticket, out4);
+  }
 }
 
 }  // namespace chll

@@ -112,6 +112,8 @@ struct UnitNbhd {
   float4 n0, n1;
   Nbrs nb0, nb1;
   bool v0, v1;
+  // presence of the forward neighbours: +x of each site, +y, +z
+  bool fx0, fx1, fy, fz;
 };
 
 template <int C, bool PXY, bool PZ>
@@ -157,6 +159,10 @@ __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeo
     if (!hkp) skp = rs - (nk - 1) * plane;
     hkm = hkp = true;
   }
+  U.fx0 = hxb;
+  U.fx1 = hxc;
+  U.fy = hjp;
+  U.fz = hkp;
   const float4* orow = oth + rs;
   const float4 fa = hxa ? ld4(orow + (xa >> 1)) : zero;
   const float4 fb = hxb ? ld4(orow + (xb >> 1)) : zero;

@@ -69,3 +69,50 @@ def test_noalloc_adjoint_refuses_lattices_beyond_its_scratch():
     assert rc == _lib.CHLL_ERANGE
     assert "at most 262144" in _lib.last_error()
     lat.close()
+
+
+def test_noalloc_adjoint_on_16_byte_aligned_arrays():
+    """Caller arrays that start 16 but not 32 bytes aligned (a float4 array
+    at an odd slot) take the one-slot-per-thread kernel, with the same
+    results as the library's own 32-byte aligned storage."""
+    import torch
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    L = _lib.load()
+    shape = (20, 18, 10)
+    lat = Lattice(*shape, boundary="periodic")
+    lat.init_random(seed=8)
+    cp = coupling(0.3, 1.0, 0.5, 1.1)
+    lat.set_control(0.1, step=1)
+    lat.sweep(cp, 3, seed=8)
+    ref_grad, ref_out4 = lat.energy_grad(cp, project=True)
+    c0, c1, per_colour, _ = lat.storage()
+    # copies of both colour arrays one float4 past a 256-byte aligned start
+    buf = torch.empty((2, per_colour + 2, 4), dtype=torch.float32, device="cuda")
+    for c, src in enumerate((c0, c1)):
+        view = torch.as_tensor(_DeviceF4(src, per_colour), device="cuda")
+        buf[c, 1:per_colour + 1].copy_(view)
+    p0, p1 = buf[0, 1:].data_ptr(), buf[1, 1:].data_ptr()
+    assert p0 % 32 == 16 and p1 % 32 == 16
+    n = lat.nsites
+    grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    out4 = torch.empty(4, dtype=torch.float64, device="cuda")
+    rc = L.chll_energy_grad_noalloc(ct.c_void_p(p0), ct.c_void_p(p1), *shape, _lib.CHLL_PERIODIC,
+                                    ct.byref(cp), 1, ct.c_void_p(grad.data_ptr()),
+                                    ct.c_void_p(out4.data_ptr()),
+                                    ct.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(grad.cpu().numpy(), ref_grad, rtol=GRAD_RTOL, atol=GRAD_ATOL)
+    np.testing.assert_allclose(out4.cpu().numpy(), ref_out4, rtol=SUM_RTOL, atol=SUM_RTOL)
+    lat.close()
+
+
+class _DeviceF4:
+    """(count, 4) float32 device array at an address, for torch.as_tensor."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (count, 4), "typestr": "<f4",
+                                         "data": (ptr, False), "version": 3, "strides": None}
