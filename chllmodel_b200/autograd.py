@@ -3,7 +3,7 @@
 ``lattice_energy(n, s, eps, K, h, shape, boundary)`` returns the FP64 total
 energy of a lattice whose directors ``n`` (N x 3, FP32, CUDA, natural order
 i fastest) and chiralities ``s`` (N, +-1) are torch tensors; its backward
-pass comes from ``energy_grad_kernel`` (dE/dn for every site, plus
+pass comes from the adjoint kernel (``energy_grad_unit_kernel``: dE/dn for every site, plus
 dE/deps, dE/dK, dE/dh in FP64), not from autograd tracing.  The Metropolis
 sweep itself is not differentiated: acceptance stays exactly the reference's
 rule (chll_mod.f90:188-200).
