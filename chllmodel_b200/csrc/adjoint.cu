@@ -13,6 +13,7 @@
 // Coupling derivatives (FP64): dE/deps = sum(1-c^2), dE/dK = -sum(c*X*sbar),
 // dE/dh = -sum(s), together with E itself.
 #include <algorithm>
+#include <atomic>
 
 #include "chll_common.cuh"
 #include "moments.cuh"
@@ -293,17 +294,20 @@ __global__ void __launch_bounds__(kGradThreads) quench_pass_kernel(LatticeView L
 }
 
 // CTAs of `kernel` (kGradThreads threads) resident on the current device, one
-// wave of a grid-stride launch; cached per device ordinal.
+// wave of a grid-stride launch; cached per device ordinal (threads that race
+// on the first query store the same value).
 template <class Kernel>
-int resident_ctas(Kernel kernel, int cache[16]) {
+int resident_ctas(Kernel kernel, std::atomic<int> cache[16]) {
   int dev = 0;
   cudaGetDevice(&dev);
-  int& res = cache[dev & 15];
+  std::atomic<int>& slot = cache[dev & 15];
+  int res = slot.load(std::memory_order_relaxed);
   if (res == 0) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kGradThreads, 0);
     res = std::max(1, sms) * std::max(1, per_sm);
+    slot.store(res, std::memory_order_relaxed);
   }
   return res;
 }
@@ -319,7 +323,7 @@ void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, in
   cp.K = (float)cd.K;
   cp.g = (float)cd.g;
   cp.inv_kT = 0.f;
-  static int resident[16] = {0};
+  static std::atomic<int> resident[16];
   const int res = resident_ctas(quench_pass_kernel<0, true>, resident);
   const SweepGeom G = make_geom(L);
   size_t blocks = ((size_t)G.units + kGradThreads - 1) / kGradThreads;
@@ -340,7 +344,7 @@ void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_
                         cudaStream_t stream) {
   const size_t total = 2 * (size_t)L.nk * L.nj * L.hx;
   const bool units = unit_view_aligned(L) && ((uintptr_t)grad_rb % 32) == 0;
-  static int resident[16] = {0};
+  static std::atomic<int> resident[16];
   const int res = units ? resident_ctas(energy_grad_unit_kernel<true>, resident) : kGradMaxBlocks;
   size_t blocks = ((units ? total / 4 : total) + kGradThreads - 1) / kGradThreads;
   if (blocks > (size_t)std::min(res, kGradMaxBlocks)) blocks = std::min(res, kGradMaxBlocks);
