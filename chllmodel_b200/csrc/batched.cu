@@ -176,10 +176,14 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   const Coupling cp = D.cp;
   const PhiloxKeys key = philox_keys(D.key0, D.key1);
   const uint32_t replica = D.replica;
-  for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units;
-       g += (uint32_t)nct * THREADS)
+  const uint32_t stride = (uint32_t)nct * THREADS;
+  const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
+  const uint32_t per_colour = plane * (uint32_t)L.nk;
+  for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units; g += stride) {
+    if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
     unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, step, d, cp, key,
                                                                    replica, nacc, nflip);
+  }
 }
 
 template <int PHASE, int THREADS>

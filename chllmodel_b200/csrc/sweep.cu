@@ -86,8 +86,11 @@ __global__ void __launch_bounds__(kThreads, 3)
   const long long step = ctl->step;
   const float d = (float)ctl->d;
   unsigned int accepted = 0;
-  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units;
-       g += gridDim.x * kThreads) {
+  const uint32_t stride = gridDim.x * kThreads;
+  const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
+  const uint32_t per_colour = plane * (uint32_t)L.nk;
+  for (uint32_t g = blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
+    if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
     accepted += sweep_unit<DIRECTOR, C, PERIODIC>(L, G, g, (uint32_t)step, d, cp, key0, key1,
                                                   replica);
   }
@@ -182,8 +185,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   const long long step = ctl->step;
   const float d = (float)ctl->d;
   unsigned int nacc = 0, nflip = 0;
-  for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units;
-       g += gridDim.x * kThreads) {
+  const uint32_t stride = gridDim.x * kThreads;
+  const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
+  const uint32_t per_colour = plane * (uint32_t)L.nk;
+  for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
+    if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
     unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
                                                         replica, nacc, nflip);
   }
