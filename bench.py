@@ -40,9 +40,9 @@ BATCH_NOUT = 50
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
-# B) on a 256^3 launch and scaled by sites to 480^3: 369.9 MB (A) and
-# 370.4 MB (B) per launch of 16.78 M sites.
-TRAFFIC_BYTES_PER_SITE_PASS = 22.06
+# B) on a 256^3 launch and scaled by sites to 480^3: 370.6 MB (A) and
+# 372.1 MB (B) per launch of 16.78 M sites.
+TRAFFIC_BYTES_PER_SITE_PASS = 22.14
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
