@@ -33,12 +33,24 @@ EXPORTS = (
     "chll_lattice_read_rows", "chll_energy_grad_noalloc", "chll_lattice_quench",
     "chll_lattice_set_kernel", "chll_lattice_shell_corr", "chll_lattice_projection",
     "chll_lattice_create_slab", "chll_lattice_slab_plane", "chll_lattice_counters",
-    "chll_lattice_control_update",
+    "chll_lattice_control_update", "chll_lattice_slab_set_peers", "chll_lattice_slab_push",
+    "chll_lattice_ipc_handle", "chll_ipc_open", "chll_ipc_close",
     "chll_batch_create", "chll_batch_destroy", "chll_batch_set_stream", "chll_batch_sync",
     "chll_batch_init_random", "chll_batch_upload_f4", "chll_batch_download_f4", "chll_batch_run",
     "chll_batch_moments", "chll_batch_info", "chll_batch_set_tuning", "chll_batch_autotune",
     "chll_batch_set_wave_bytes", "chll_batch_get_tuning",
 )
+
+
+def torch_stream_handle(stream=None) -> int:
+    """The CUDA stream handle of a torch stream (default: the current one) for
+    the set_stream calls: torch's default stream is handle 0, which the
+    library reads as "the lattice's own stream", so it becomes
+    cudaStreamLegacy (1), the same default stream by its explicit name."""
+    import torch
+
+    h = (stream if stream is not None else torch.cuda.current_stream()).cuda_stream
+    return h if h else 1
 
 
 class ChllError(RuntimeError):
@@ -149,8 +161,15 @@ def _declare(L: ct.CDLL) -> None:
     L.chll_lattice_slab_plane.argtypes = [vp, i32, i32, P(vp), P(i64)]
     L.chll_lattice_counters.argtypes = [vp, P(vp)]
     L.chll_lattice_control_update.argtypes = [vp, i32]
+    L.chll_lattice_slab_set_peers.argtypes = [vp, vp, vp, vp, vp]
+    L.chll_lattice_slab_push.argtypes = [vp, i32]
+    L.chll_lattice_ipc_handle.argtypes = [vp, vp, P(u64)]
+    L.chll_ipc_open.argtypes = [vp, P(vp)]
+    L.chll_ipc_close.argtypes = [vp]
     for name in ("chll_lattice_create_slab", "chll_lattice_slab_plane", "chll_lattice_counters",
-                 "chll_lattice_control_update"):
+                 "chll_lattice_control_update", "chll_lattice_slab_set_peers",
+                 "chll_lattice_slab_push", "chll_lattice_ipc_handle", "chll_ipc_open",
+                 "chll_ipc_close"):
         getattr(L, name).restype = i32
     L.chll_lattice_shell_corr.argtypes = [vp, i32, i32, vp, vp, vp]
     L.chll_lattice_shell_corr.restype = i32

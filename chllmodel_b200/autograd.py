@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import torch
 
+from . import _lib
 from .lattice import Lattice, coupling
 
 _cache: dict = {}
@@ -32,8 +33,7 @@ def _lattice(shape, boundary, device) -> Lattice:
 
 
 def _stream_handle() -> int:
-    h = torch.cuda.current_stream().cuda_stream
-    return h if h else 1  # cudaStreamLegacy for torch's default stream
+    return _lib.torch_stream_handle()
 
 
 def _pack(n: torch.Tensor, s: torch.Tensor) -> torch.Tensor:

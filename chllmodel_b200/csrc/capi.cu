@@ -163,6 +163,10 @@ struct chll_lattice {
   // plane 0 keeps the storage checkerboard equal to the global one).
   int slab = 0, z0 = 0, nk_global = 0;
   long long ctl_sites = 0;  // sites of the whole lattice (acceptance fractions)
+  // where a slab's first / last own plane of each colour is also written by
+  // its passes (the neighbouring slabs' halo planes), or null
+  float4* peer_lo[2] = {nullptr, nullptr};
+  float4* peer_hi[2] = {nullptr, nullptr};
 
   int store_planes() const { return slab ? nk + 3 : nk; }
   // The lattice's own sites (a slab's interior planes).
@@ -825,9 +829,10 @@ int chll_lattice_pass(chll_lattice* L, const chll_coupling* c, uint64_t seed, ui
     if (pass < 4) return fail(CHLL_EINVAL, "pass: a slab runs the fused passes 4..7 only");
     const LatticeView sv = L->store_view();
     const chll::SweepGeom G = chll::make_slab_geom(sv, 2, L->nk, L->z0 - 2);
+    const int colour = pass == 4 + chll::kFusedB ? 1 : 0;
     chll::launch_fused_pass(sv, G, L->periodic ? chll::kBoundSlabXY : chll::kBoundOpen,
                             make_coupling(*c), seed_lo(seed), seed_hi(seed), replica, L->ctl,
-                            pass - 4, L->stream);
+                            pass - 4, L->stream, L->peer_lo[colour], L->peer_hi[colour]);
     CHLL_CUDA_TRY(cudaGetLastError());
     return ok();
   }
@@ -1064,6 +1069,66 @@ static_assert(offsetof(Control, nflip) == offsetof(Control, nacc) + sizeof(unsig
 int chll_lattice_counters(chll_lattice* L, void** ptr) {
   if (!L || !ptr) return fail(CHLL_EINVAL, "counters: null argument");
   *ptr = &L->ctl->nacc;  // {nacc, nflip}: two consecutive uint64
+  return ok();
+}
+
+int chll_lattice_slab_set_peers(chll_lattice* L, void* lower0, void* lower1, void* upper0,
+                                void* upper1) {
+  if (!L) return fail(CHLL_EINVAL, "null lattice");
+  if (!L->slab) return fail(CHLL_EINVAL, "slab_set_peers: not a slab");
+  void* const p[4] = {lower0, lower1, upper0, upper1};
+  for (void* q : p) {
+    if (!q) continue;
+    if ((uintptr_t)q % 32)
+      return fail(CHLL_EINVAL, "slab_set_peers: %p is not 32-byte aligned (a halo plane of a "
+                  "slab from chll_lattice_slab_plane is)", q);
+    if (!is_device_ptr(q))
+      return fail(CHLL_EINVAL, "slab_set_peers: %p is not device memory", q);
+  }
+  CHLL_CUDA_TRY(cudaStreamSynchronize(L->stream));
+  L->peer_lo[0] = (float4*)lower0;
+  L->peer_lo[1] = (float4*)lower1;
+  L->peer_hi[0] = (float4*)upper0;
+  L->peer_hi[1] = (float4*)upper1;
+  return ok();
+}
+
+int chll_lattice_slab_push(chll_lattice* L, int colour) {
+  if (!L) return fail(CHLL_EINVAL, "null lattice");
+  if (!L->slab) return fail(CHLL_EINVAL, "slab_push: not a slab");
+  if (colour < 0 || colour > 1) return fail(CHLL_EINVAL, "slab_push: colour 0 or 1");
+  const size_t per_plane = (size_t)L->hx * L->nj;
+  const float4* base = L->lat + (size_t)colour * L->per_colour;
+  if (L->peer_lo[colour])
+    CHLL_CUDA_TRY(cudaMemcpyAsync(L->peer_lo[colour], base + 2 * per_plane,
+                                  per_plane * sizeof(float4), cudaMemcpyDefault, L->stream));
+  if (L->peer_hi[colour])
+    CHLL_CUDA_TRY(cudaMemcpyAsync(L->peer_hi[colour], base + (size_t)(L->nk + 1) * per_plane,
+                                  per_plane * sizeof(float4), cudaMemcpyDefault, L->stream));
+  return ok();
+}
+
+int chll_lattice_ipc_handle(chll_lattice* L, void* handle64, uint64_t* base) {
+  if (!L || !handle64 || !base) return fail(CHLL_EINVAL, "ipc_handle: null argument");
+  static_assert(sizeof(cudaIpcMemHandle_t) == 64, "the ABI passes 64-byte IPC handles");
+  cudaIpcMemHandle_t h;
+  CHLL_CUDA_TRY(cudaIpcGetMemHandle(&h, L->lat));
+  std::memcpy(handle64, &h, sizeof(h));
+  *base = (uint64_t)(uintptr_t)L->lat;
+  return ok();
+}
+
+int chll_ipc_open(const void* handle64, void** ptr) {
+  if (!handle64 || !ptr) return fail(CHLL_EINVAL, "ipc_open: null argument");
+  cudaIpcMemHandle_t h;
+  std::memcpy(&h, handle64, sizeof(h));
+  CHLL_CUDA_TRY(cudaIpcOpenMemHandle(ptr, h, cudaIpcMemLazyEnablePeerAccess));
+  return ok();
+}
+
+int chll_ipc_close(void* ptr) {
+  if (!ptr) return fail(CHLL_EINVAL, "ipc_close: null pointer");
+  CHLL_CUDA_TRY(cudaIpcCloseMemHandle(ptr));
   return ok();
 }
 

@@ -172,10 +172,13 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 // Two CTAs per SM: the two sites' interleaved trials want up to 128
 // registers, and measured, 2 x 256 threads run these passes faster than 3 x 256
 // at 80 registers.
+// peer: the halo planes of neighbouring z-slabs that this slab's boundary
+// planes are written to (null pointers for a whole lattice).  The periodic
+// whole-lattice mode has no peers.
 template <int PHASE, int BMODE>
 __global__ void __launch_bounds__(kThreads, 2)
     fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, PhiloxKeys keys,
-                      uint32_t replica, Control* __restrict__ ctl) {
+                      uint32_t replica, Control* __restrict__ ctl, PeerPlanes peer) {
   constexpr int C = PHASE == kFusedB ? 1 : 0;
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
   constexpr bool DIR = PHASE != kFusedF;
@@ -188,10 +191,20 @@ __global__ void __launch_bounds__(kThreads, 2)
   const uint32_t stride = gridDim.x * kThreads;
   const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
   const uint32_t per_colour = plane * (uint32_t)L.nk;
-  for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
-    if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-    unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
-                                                        replica, nacc, nflip);
+  if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
+    for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
+      if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
+      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
+                                                          replica, nacc, nflip);
+    }
+  } else {
+    for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
+      if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
+      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
+                                                          replica, nacc, nflip, peer);
+    }
+    // the halo stores reach the other GPU before this kernel counts as done
+    __threadfence_system();
   }
   fused_epilogue<PHASE>(ctl, nacc, nflip, step);
 }
@@ -246,7 +259,8 @@ const StagedKernel kStaged[2][4] = {
     {staged_pass_kernel<true, 0, true>, staged_pass_kernel<true, 1, true>,
      staged_pass_kernel<false, 0, true>, staged_pass_kernel<false, 1, true>}};
 
-using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*);
+using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*,
+                            PeerPlanes);
 
 // [boundary mode][phase]
 const FusedKernel kFused[3][4] = {
@@ -357,15 +371,23 @@ void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, 
 
 void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, const Coupling& cp,
                        uint32_t key0, uint32_t key1, uint32_t replica, Control* ctl, int phase,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, float4* peer_lo, float4* peer_hi) {
   DeviceShape& ds = device_shape();
   const int m = bmode < 0 ? 0 : (bmode > 2 ? 2 : bmode);
   const uint32_t n = G.units - G.first;
   const uint32_t need = (n + kThreads - 1) / kThreads;
   const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3];
   const dim3 grid(need < resident ? (need ? need : 1) : resident);
+  // The first and last planes of the unit range: slots 2*first .. and the
+  // plane before slot 2*units.
+  PeerPlanes peer;
+  peer.plane = (uint32_t)L.hx * (uint32_t)L.nj;
+  peer.lo = m == kBoundPeriodic ? nullptr : peer_lo;
+  peer.hi = m == kBoundPeriodic ? nullptr : peer_hi;
+  peer.lo_first = 2 * G.first;
+  peer.hi_first = 2 * G.units - peer.plane;
   kFused[m][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1), replica,
-                                                       ctl);
+                                                       ctl, peer);
 }
 
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,

@@ -26,11 +26,14 @@ enum FusedPhase : int { kFusedA0 = 0, kFusedA = 1, kFusedB = 2, kFusedF = 3 };
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int phase, cudaStream_t stream);
 // The same on an explicit unit range and boundary mode (sweep_unit.cuh:
-// make_slab_geom, BoundaryMode), for a z-slab with halo planes.
+// make_slab_geom, BoundaryMode), for a z-slab with halo planes.  peer_lo /
+// peer_hi: where the range's first / last plane is also written (the halo
+// planes of the neighbouring slabs, 32-byte aligned), or null.
 struct SweepGeom;
 void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, const Coupling& cp,
                        uint32_t key0, uint32_t key1, uint32_t replica, Control* ctl, int phase,
-                       cudaStream_t stream);
+                       cudaStream_t stream, float4* peer_lo = nullptr,
+                       float4* peer_hi = nullptr);
 // The control update of a fused pass when the control block defers it.
 void launch_control_update(Control* ctl, int phase, cudaStream_t stream);
 

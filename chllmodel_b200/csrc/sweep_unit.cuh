@@ -192,19 +192,43 @@ __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeo
   nbr_units(hkm, oth + skm + h0, U.nb0.b[5], U.nb1.b[5]);
 }
 
+// Where else an updated unit is written: nowhere (whole lattices), or, for a
+// z-slab, into the neighbouring slabs' halo planes.
+struct NoPeer {
+  __device__ __forceinline__ void store(uint32_t, const float4&, const float4&) const {}
+};
+
+// A slab's first and last own planes of the pass's colour also go straight
+// into the halo planes of the slabs below (lo) and above (hi): slots
+// [lo_first, lo_first + plane) to lo + (slot - lo_first), likewise for hi.
+// lo / hi are 32-byte aligned device addresses (another GPU's memory through
+// an IPC mapping, or another slab's on this GPU), or null.
+struct PeerPlanes {
+  float4* lo;
+  float4* hi;
+  uint32_t lo_first, hi_first, plane;
+  __device__ __forceinline__ void store(uint32_t slot, const float4& n0, const float4& n1) const {
+    if (lo && slot - lo_first < plane) st_unit(lo + (slot - lo_first), n0, n1);
+    if (hi && slot - hi_first < plane) st_unit(hi + (slot - hi_first), n0, n1);
+  }
+};
+
 // Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
-// and accepted flips to nflip.
-template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY>
+// and accepted flips to nflip.  A unit's slots are 2g (rows of hx = 2Q).
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY,
+          class PEER = NoPeer>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica,
-                                          unsigned int& nacc, unsigned int& nflip) {
+                                          unsigned int& nacc, unsigned int& nflip,
+                                          const PEER& peer = PEER()) {
   UnitNbhd U;
   gather_unit<C, PXY, PZ>(L, G, g, U);
   unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(U.n0, U.n1, U.nb0, U.nb1, U.v0, U.v1, g + G.goff,
                                                step, d, cp, key, replica, nacc, nflip);
   st_unit(U.cen, U.n0, U.n1);
+  peer.store(2 * g, U.n0, U.n1);
 }
 
 // One of the reference's four half-sweeps on unit g; returns the number of

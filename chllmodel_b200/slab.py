@@ -15,7 +15,9 @@ A halo exchange moves one plane of one colour (hx*nj float4) to each
 neighbouring slab; a count sum is a 64-bit all-reduce.  ``LocalHalo`` does both
 for slabs held by this process (device-to-device copies on one stream);
 ``TorchHalo`` does them with ``torch.distributed`` (NCCL between GPUs, or gloo
-with host tensors) for one slab per rank.
+with host tensors) for one slab per rank.  ``PeerHalo`` (one process) and
+``TorchPeerHalo`` (one slab per rank, CUDA IPC) move no planes between passes:
+the passes themselves store the boundary planes into the neighbours' halos.
 """
 from __future__ import annotations
 
@@ -76,6 +78,26 @@ class SlabLattice(Lattice):
     def control_update(self, code: int) -> None:
         check(self._L.chll_lattice_control_update(self._h, int(code)))
 
+    def set_peers(self, lower=(None, None), upper=(None, None)) -> None:
+        """From now on every pass of colour c also writes this slab's first own
+        plane to the device address lower[c] and its last own plane to
+        upper[c]: the upper halo of the slab below and the lower halo of the
+        slab above (None: no neighbour on that side)."""
+        v = lambda a: ct.c_void_p(a) if a else None
+        check(self._L.chll_lattice_slab_set_peers(self._h, v(lower[0]), v(lower[1]), v(upper[0]),
+                                                  v(upper[1])))
+
+    def push(self, colour: int) -> None:
+        """Copies the own boundary planes of one colour to the peers."""
+        check(self._L.chll_lattice_slab_push(self._h, int(colour)))
+
+    def ipc_handle(self) -> tuple[bytes, int]:
+        """(64-byte CUDA IPC handle of the lattice allocation, its base address)."""
+        buf = ct.create_string_buffer(64)
+        base = ct.c_uint64()
+        check(self._L.chll_lattice_ipc_handle(self._h, buf, ct.byref(base)))
+        return buf.raw, base.value
+
 
 class _DeviceArray:
     """A device address as a __cuda_array_interface__ object (zero-copy view)."""
@@ -127,6 +149,32 @@ class LocalHalo:
             t[index:index + 1].copy_(total)
 
 
+class PeerHalo(LocalHalo):
+    """Slabs held by this process whose passes write their boundary planes
+    straight into the neighbouring slabs' halo planes (set_peers), so no copy
+    is left between passes: the single stream orders the passes.  Count sums
+    as LocalHalo."""
+
+    def __init__(self, slabs: list[SlabLattice]):
+        super().__init__(slabs)
+        n = len(self.slabs)
+        for r, sl in enumerate(self.slabs):
+            down = r - 1 if r > 0 else (n - 1 if self.periodic else None)
+            up = r + 1 if r + 1 < n else (0 if self.periodic else None)
+            lower = [self.slabs[down].plane(c, UPPER_HALO)[0] if down is not None else None
+                     for c in (0, 1)]
+            upper = [self.slabs[up].plane(c, LOWER_HALO)[0] if up is not None else None
+                     for c in (0, 1)]
+            sl.set_peers(lower, upper)
+
+    def prime(self, colour: int) -> None:
+        for sl in self.slabs:
+            sl.push(colour)
+
+    def exchange(self, colour: int) -> None:
+        pass  # written by the passes themselves
+
+
 class TorchHalo:
     """Halo exchange and count sums with torch.distributed, one slab per rank.
     `planes(colour, which)` and `counts` are this rank's tensors (device tensors
@@ -148,9 +196,7 @@ class TorchHalo:
         """The transport of `slab`, which from here on launches on the current
         CUDA stream: torch orders its NCCL operations after that stream's
         work, so passes and exchanges stay in order."""
-        import torch
-
-        slab.set_stream(torch.cuda.current_stream().cuda_stream)
+        slab.set_stream(_lib.torch_stream_handle())
         planes = {(c, w): _plane_tensor(slab, c, w) for c in (0, 1) for w in range(4)}
         return cls(lambda c, w: planes[(c, w)], _counter_tensor(slab),
                    slab.boundary == "periodic", group)
@@ -192,16 +238,111 @@ class TorchHalo:
         self.dist.all_reduce(self.counts[index:index + 1], group=self.group)
 
 
+class TorchPeerHalo(TorchHalo):
+    """One slab per rank, halos written inside the passes over peer memory.
+
+    Each rank maps its neighbours' lattice allocations (CUDA IPC,
+    chll_lattice_ipc_handle / chll_ipc_open, exchanged with all_gather) and
+    sets their halo planes as its slab's peers: a pass of colour c writes the
+    slab's boundary planes of colour c into the neighbours' halos as it
+    updates them (one 256-bit store per boundary unit, over NVLink between
+    GPUs).  Between passes only the ordering is left, and it comes from the
+    collectives that follow every pass: the count all-reduce, or a
+    one-element all-reduce after a pass that closes no count (exchange()).
+    Every rank's next pass starts after every rank's previous pass, so a
+    halo is never written while it is read.  With NCCL the collectives are
+    ordered on the current stream; with gloo (tests: processes sharing one
+    GPU) the device is synchronised around them.  No kernel waits on
+    another GPU."""
+
+    def __init__(self, slab: SlabLattice, group=None):
+        import torch
+        import torch.distributed as dist
+
+        slab.set_stream(_lib.torch_stream_handle())
+        super().__init__(None, _counter_tensor(slab), slab.boundary == "periodic", group)
+        self.slab = slab
+        self.gloo = dist.get_backend(group) == "gloo"
+        handle, base = slab.ipc_handle()
+        offs = {(c, w): slab.plane(c, w)[0] - base for c in (0, 1)
+                for w in (LOWER_HALO, UPPER_HALO)}
+        info = [None] * self.world
+        dist.all_gather_object(info, (handle, offs), group=group)
+        down, up = self._neighbours()
+        self._mapped = {}
+
+        def base_of(r):
+            if r == self.rank:
+                return base
+            if r not in self._mapped:
+                p = ct.c_void_p()
+                check(slab._L.chll_ipc_open(info[r][0], ct.byref(p)))
+                self._mapped[r] = p.value
+            return self._mapped[r]
+
+        lower = [base_of(down) + info[down][1][(c, UPPER_HALO)] if down is not None else None
+                 for c in (0, 1)]
+        upper = [base_of(up) + info[up][1][(c, LOWER_HALO)] if up is not None else None
+                 for c in (0, 1)]
+        slab.set_peers(lower, upper)
+        self._token = torch.zeros(1, dtype=torch.int64,
+                                  device="cpu" if self.gloo else "cuda")
+
+    @classmethod
+    def for_slab(cls, slab: SlabLattice, group=None):
+        return cls(slab, group)
+
+    def _all_reduce(self, t) -> None:
+        import torch
+
+        if self.gloo:
+            torch.cuda.current_stream().synchronize()
+            host = t.cpu() if t.is_cuda else t
+            self.dist.all_reduce(host, group=self.group)
+            if t.is_cuda:
+                t.copy_(host)
+                torch.cuda.current_stream().synchronize()
+        else:
+            self.dist.all_reduce(t, group=self.group)
+
+    def prime(self, colour: int) -> None:
+        self._all_reduce(self._token)   # neighbours' previous passes are done
+        self.slab.push(colour)
+        self._all_reduce(self._token)   # and every halo is filled
+
+    def exchange(self, colour: int) -> None:
+        self._all_reduce(self._token)
+
+    def sum_counts(self, index: int) -> None:
+        self._all_reduce(self.counts[index:index + 1])
+
+    def close(self) -> None:
+        """Unmaps the neighbours' allocations after the last pass; collective
+        (every rank calls it before freeing its slab)."""
+        import torch
+
+        torch.cuda.current_stream().synchronize()
+        self._all_reduce(self._token)   # no rank still writes into a mapped halo
+        self.slab.set_peers()
+        for p in self._mapped.values():
+            check(self.slab._L.chll_ipc_close(ct.c_void_p(p)))
+        self._mapped = {}
+        torch.cuda.current_stream().synchronize()
+        self._all_reduce(self._token)   # every mapping of this slab is gone before it is freed
+
+
 def sweep_slabs(slabs: list[SlabLattice], halo, cp, nsweeps: int, seed: int = 1,
                 replica: int = 0) -> None:
     """nsweeps fused sweeps of the slabs held here, exchanging halos through
-    `halo` (LocalHalo or TorchHalo); every slab ends with all trials done.
-    The slabs must launch on the stream that is current while this runs (the
-    halo copies and collectives are ordered on it)."""
+    `halo` (LocalHalo, PeerHalo, TorchHalo or TorchPeerHalo); every slab ends
+    with all trials done.  The slabs must launch on the stream that is
+    current while this runs (the halo copies and collectives are ordered on
+    it)."""
     if nsweeps <= 0:
         return
-    halo.exchange(0)
-    halo.exchange(1)
+    prime = getattr(halo, "prime", halo.exchange)  # the halos' first fill
+    prime(0)
+    prime(1)
     for s in range(nsweeps):
         for sl in slabs:
             sl.half_sweep(cp, FUSED_A if s else FUSED_A0, seed, replica)

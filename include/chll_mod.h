@@ -284,6 +284,27 @@ int chll_lattice_counters(chll_lattice* lat, void** ptr);
 /* The control update that pass `pass` (4..7) defers on a slab: 5 and 7 close
  * the previous step's flip fraction, 6 the director fraction, d and the step. */
 int chll_lattice_control_update(chll_lattice* lat, int pass);
+/* Halo exchange inside the passes: every fused pass of colour c also writes
+ * the slab's first own plane to lower_c and its last own plane to upper_c
+ * (the upper halo of the slab below and the lower halo of the slab above),
+ * so no separate exchange is needed between passes, only the ordering that
+ * the count sums already give.  NULL = no such neighbour.  32-byte aligned
+ * device addresses this GPU can store to: another slab's plane on this GPU
+ * (chll_lattice_slab_plane) or a neighbouring GPU's, mapped with
+ * chll_ipc_open.  Replaces the caller's halo copies (slab.py TorchHalo). */
+int chll_lattice_slab_set_peers(chll_lattice* lat, void* lower0, void* lower1, void* upper0,
+                                void* upper1);
+/* Copies the first and last own planes of colour `colour` to the peers set
+ * above (the halo fill before the first pass). */
+int chll_lattice_slab_push(chll_lattice* lat, int colour);
+/* IPC export of the lattice's device allocation: the 64-byte
+ * cudaIpcMemHandle_t into handle64 and the allocation's address in this
+ * process (a plane's offset in it = its address - base). */
+int chll_lattice_ipc_handle(chll_lattice* lat, void* handle64, uint64_t* base);
+/* Maps an allocation exported by another process (chll_lattice_ipc_handle)
+ * into this one: *ptr = its base here.  chll_ipc_close unmaps it. */
+int chll_ipc_open(const void* handle64, void** ptr);
+int chll_ipc_close(void* ptr);
 
 /* ---- Analysis (the reference's notebook analyses, on the device) ---------- */
 

@@ -1,23 +1,29 @@
 """z-slabs on one GPU: a lattice split into slabs that exchange halo planes
-between passes (LocalHalo) follows the whole lattice's chain bit for bit, and
-the slabs' measurement rows add up to the whole lattice's."""
+between passes (LocalHalo) or write them into each other's halos during the
+passes (PeerHalo) follows the whole lattice's chain bit for bit, and the
+slabs' measurement rows add up to the whole lattice's."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("transport", ["copies", "peer"])
 @pytest.mark.parametrize("shape,boundary,parts", [((16, 12, 16), "periodic", 2),
                                                   ((16, 12, 16), "periodic", 4),
                                                   ((12, 10, 12), "open", 3),
                                                   ((9, 6, 10), "open", 2),
-                                                  ((8, 8, 6), "periodic", 3)])
-def test_slabs_follow_the_whole_lattice(shape, boundary, parts):
+                                                  ((8, 8, 6), "periodic", 3),
+                                                  ((8, 8, 6), "periodic", 1)])
+def test_slabs_follow_the_whole_lattice(shape, boundary, parts, transport):
+    """transport "copies": LocalHalo copies the boundary planes between
+    passes; "peer": PeerHalo, the passes write them into the neighbours'
+    halos themselves (one periodic slab is its own neighbour)."""
     import torch
 
     from chllmodel_b200.lattice import Lattice, coupling
-    from chllmodel_b200.slab import LocalHalo, SlabLattice, slab_observables, split_planes, \
-        sweep_slabs
+    from chllmodel_b200.slab import LocalHalo, PeerHalo, SlabLattice, slab_observables, \
+        split_planes, sweep_slabs
 
     ni, nj, nk = shape
     cp = coupling(0.6, 1.0, 0.2, 1.1)
@@ -40,7 +46,7 @@ def test_slabs_follow_the_whole_lattice(shape, boundary, parts):
         sl.set_control(0.15, step=1)
         slabs.append(sl)
     with torch.cuda.stream(s):
-        halo = LocalHalo(slabs)
+        halo = LocalHalo(slabs) if transport == "copies" else PeerHalo(slabs)
         sweep_slabs(slabs, halo, cp, 4, seed=5, replica=2)
         sweep_slabs(slabs, halo, cp, nsw - 4, seed=5, replica=2)
     s.synchronize()
