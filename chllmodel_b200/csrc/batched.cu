@@ -613,11 +613,6 @@ int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
   if (!out) return fail(CHLL_EINVAL, "batch_create: null output pointer");
   *out = nullptr;
   if (!specs || n <= 0) return fail(CHLL_EINVAL, "batch_create: need at least one replica");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return fail(CHLL_ECUDA, "no CUDA device available; libchll_mod has no CPU path");
-  }
   for (int r = 0; r < n; ++r) {
     const chll_replica_spec& s = specs[r];
     if (s.ni < 1 || s.nj < 1 || s.nk < 1)
@@ -628,8 +623,14 @@ int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
       return fail(CHLL_EINVAL, "batch_create: replica %d is periodic with odd dims", r);
     if (!(s.kT >= 0.0)) return fail(CHLL_EINVAL, "batch_create: replica %d has kT < 0", r);
     const long long units = (long long)(chll::padded_ni(s.ni) / 4) * s.nj * s.nk;
-    if (units >= (1LL << 31))
-      return fail(CHLL_EINVAL, "batch_create: replica %d is too large", r);
+    if (units >= (1LL << 30))  // 2 slots per unit: < 2^31 slots per colour
+      return fail(CHLL_EINVAL, "batch_create: replica %d is too large (%lld units, limit 2^30)",
+                  r, units);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CHLL_ECUDA, "no CUDA device available; libchll_mod has no CPU path");
   }
   chll::sweep_prepare();
   chll_batch* B = new chll_batch();

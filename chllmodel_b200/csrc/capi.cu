@@ -387,6 +387,15 @@ int create_impl(int ni, int nj, int nk, int boundary, chll_lattice** out, int sl
   const long long groups = (long long)(chll::padded_ni(ni) / 4) * nj * nk;
   if (n >= (1LL << 32) || groups >= (1LL << 32))
     return fail(CHLL_EINVAL, "lattice too large for 32-bit random counters (%lld sites)", n);
+  // The kernels index the slots of one colour (padded rows, a slab's halo
+  // planes included) in 32 bits: fewer than 2^31 of them.
+  const long long planes = slab_z0 >= 0 ? (long long)slab_nk + 3 : (long long)nk;
+  const long long slots = (long long)(chll::padded_ni(ni) / 2) * nj * planes;
+  if (slots >= (1LL << 31))
+    return fail(CHLL_EINVAL,
+                "lattice too large: %lld slots per colour (rows padded to a multiple of 4 "
+                "sites%s); the limit is 2^31",
+                slots, slab_z0 >= 0 ? ", halo planes included" : "");
   CHLL_TRY(check_device());
   chll::sweep_prepare();
 

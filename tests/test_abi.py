@@ -68,6 +68,18 @@ def test_argument_validation_without_device():
     assert rc == _lib.CHLL_EINVAL
     rc = L.chll_lattice_create(8, 8, 8, 7, ct.byref(h))
     assert rc == _lib.CHLL_EINVAL
+    # 32-bit slot indices: 1 x 46341 x 46341 has < 2^32 sites, but its rows
+    # pad to 4 sites, 2^31+ slots per colour
+    rc = L.chll_lattice_create(1, 46341, 46341, _lib.CHLL_OPEN, ct.byref(h))
+    assert rc == _lib.CHLL_EINVAL and b"slots per colour" in L.chll_last_error()
+    # the whole 4 x 16384 x 65534 lattice fits; as one slab its 3 halo planes do not
+    rc = L.chll_lattice_create_slab(4, 16384, 65534, 0, 65534, _lib.CHLL_OPEN, ct.byref(h))
+    assert rc == _lib.CHLL_EINVAL and b"halo planes" in L.chll_last_error()
+    # a batch replica of 2^30 units (2^31 slots per colour) is refused before any device call
+    spec = (_lib.ReplicaSpec * 1)(_lib.ReplicaSpec(4096, 4096, 256, _lib.CHLL_PERIODIC, 1.0, 1.0,
+                                                   0.0, 1.0, 0.1, 1, 0, 0))
+    rc = L.chll_batch_create(spec, 1, ct.byref(h))
+    assert rc == _lib.CHLL_EINVAL and b"limit 2^30" in L.chll_last_error()
     cfg = _lib.RunConfig(0.5, 0.5, 0.0, 1.0, 0.1, 1, 0, 0, 10000, 0, 0)
     z = np.zeros((4, 4, 4), order="F")
     p = z.ctypes.data_as(ct.c_void_p)
