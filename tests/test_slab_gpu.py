@@ -121,3 +121,35 @@ def test_torch_halo_with_one_nccl_rank():
         sl.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_slab_peers_are_checked():
+    """set_peers takes 32-byte aligned device addresses of a slab only: a
+    misaligned or host address, or a whole lattice, is refused before any
+    pass can store to it."""
+    import ctypes as ct
+
+    import numpy as np
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import Lattice
+    from chllmodel_b200.slab import LOWER_HALO, UPPER_HALO, SlabLattice
+
+    a = SlabLattice(8, 8, 8, 0, 4, boundary="periodic")
+    b = SlabLattice(8, 8, 8, 4, 4, boundary="periodic")
+    good = b.plane(0, LOWER_HALO)[0]
+    with pytest.raises(_lib.ChllError, match="32-byte aligned"):
+        a.set_peers(upper=(good + 16, None))
+    host = np.zeros(64, np.float32)
+    host_aligned = (host.ctypes.data + 31) & ~31
+    with pytest.raises(_lib.ChllError, match="device memory"):
+        a.set_peers(upper=(host_aligned, None))
+    a.set_peers(lower=(b.plane(0, UPPER_HALO)[0], b.plane(1, UPPER_HALO)[0]),
+                upper=(good, b.plane(1, LOWER_HALO)[0]))
+    a.set_peers()
+    whole = Lattice(8, 8, 8)
+    L = _lib.load()
+    rc = L.chll_lattice_slab_set_peers(whole._h, ct.c_void_p(good), None, None, None)
+    assert rc == _lib.CHLL_EINVAL and b"not a slab" in L.chll_last_error()
+    for x in (a, b, whole):
+        x.close()
