@@ -372,8 +372,9 @@ def gpu_arm(args):
                      "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
                      "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
-                     "limiter": "instruction issue (ncu on 256^3: ~284 instructions per site, "
-                                "issue 61-63%, DRAM 39-40%); bytes are the algorithmic 24 B/site",
+                     "limiter": "instruction issue (ncu on 256^3: ~275 instructions per site, "
+                                "issue 64-65%, DRAM 41-42%, load waits hidden by an L1 prefetch); "
+                                "bytes are the algorithmic 24 B/site",
                      "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
                      "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,
                      "four_half_sweep_equiv_gbs": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)

@@ -6,8 +6,9 @@
 //
 // Work unit: the two same-colour sites of one 4-site x-block (storage slots
 // 2q, 2q+1 of a row).  A thread draws both sites' randoms from a single
-// Philox call keyed on the block and stores the pair back with two coalesced
-// 128-bit stores.  Units are numbered row-major (g = q + Q*row) and CTAs walk
+// Philox call keyed on the block and stores the pair back with one 256-bit
+// store (sweep_unit.cuh).  Units are numbered row-major (g = q + Q*row) and
+// CTAs walk
 // them grid-stride, so a launch is a few CTAs per SM that stay resident for
 // the whole pass: accept counts stay in registers and the CTA-wide reduction,
 // the one atomic and the completion ticket happen once per CTA.  All index
