@@ -8,10 +8,10 @@
 // 2q, 2q+1 of a row).  A thread draws both sites' randoms from a single
 // Philox call keyed on the block and stores the pair back with one 256-bit
 // store (sweep_unit.cuh).  Units are numbered row-major (g = q + Q*row) and
-// CTAs walk
-// them grid-stride, so a launch is a few CTAs per SM that stay resident for
-// the whole pass: accept counts stay in registers and the CTA-wide reduction,
-// the one atomic and the completion ticket happen once per CTA.  All index
+// CTAs walk them grid-stride, so a launch is a few CTAs per SM that stay
+// resident for the whole pass: accept counts stay in registers and the
+// CTA-wide reduction, the one atomic and the completion ticket happen once
+// per CTA.  All index
 // arithmetic is 32-bit (per-colour arrays < 2^31 slots); the row and plane
 // of a unit come from multiply-shift divisions.
 //
