@@ -11,9 +11,8 @@
 // CTAs walk them grid-stride, so a launch is a few CTAs per SM that stay
 // resident for the whole pass: accept counts stay in registers and the
 // CTA-wide reduction, the one atomic and the completion ticket happen once
-// per CTA.  All index
-// arithmetic is 32-bit (per-colour arrays < 2^31 slots); the row and plane
-// of a unit come from multiply-shift divisions.
+// per CTA.  All index arithmetic is 32-bit (per-colour arrays < 2^31
+// slots); the row and plane of a unit come from multiply-shift divisions.
 //
 // The last CTA to finish a pass (ticket counter) runs the step epilogue of
 // chll_mod.f90:83-93 on the device: paccept and the d adaptation after the
