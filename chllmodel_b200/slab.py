@@ -46,6 +46,14 @@ def split_planes(nk: int, parts: int) -> list[tuple[int, int]]:
     return out
 
 
+def neighbours(r: int, n: int, periodic: bool) -> tuple[int | None, int | None]:
+    """(slab below, slab above) of slab r of n along z; None past an open end.
+    A single periodic slab is its own neighbour on both sides."""
+    down = r - 1 if r > 0 else (n - 1 if periodic else None)
+    up = r + 1 if r + 1 < n else (0 if periodic else None)
+    return down, up
+
+
 class SlabLattice(Lattice):
     """Global planes z0 .. z0+nkl-1 of an ni x nj x nk lattice, with halos."""
 
@@ -134,7 +142,7 @@ class LocalHalo:
     def exchange(self, colour: int) -> None:
         n = len(self.slabs)
         for r in range(n):
-            up = r + 1 if r + 1 < n else (0 if self.periodic else None)
+            up = neighbours(r, n, self.periodic)[1]
             if up is None:
                 continue
             # my last own plane -> the next slab's lower halo, and back
@@ -159,8 +167,7 @@ class PeerHalo(LocalHalo):
         super().__init__(slabs)
         n = len(self.slabs)
         for r, sl in enumerate(self.slabs):
-            down = r - 1 if r > 0 else (n - 1 if self.periodic else None)
-            up = r + 1 if r + 1 < n else (0 if self.periodic else None)
+            down, up = neighbours(r, n, self.periodic)
             lower = [self.slabs[down].plane(c, UPPER_HALO)[0] if down is not None else None
                      for c in (0, 1)]
             upper = [self.slabs[up].plane(c, LOWER_HALO)[0] if up is not None else None
@@ -202,10 +209,7 @@ class TorchHalo:
                    slab.boundary == "periodic", group)
 
     def _neighbours(self):
-        r, n = self.rank, self.world
-        down = r - 1 if r > 0 else (n - 1 if self.periodic else None)
-        up = r + 1 if r + 1 < n else (0 if self.periodic else None)
-        return down, up
+        return neighbours(self.rank, self.world, self.periodic)
 
     def exchange(self, colour: int) -> None:
         dist = self.dist

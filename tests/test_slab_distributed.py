@@ -10,9 +10,26 @@ import torch
 import torch.multiprocessing as mp
 
 from chllmodel_b200.slab import FIRST_OWN, LAST_OWN, LOWER_HALO, UPPER_HALO, TorchHalo, \
-    split_planes
+    neighbours, split_planes
 
 PLANE = 6  # floats per fake plane
+
+
+def test_slab_neighbours():
+    """Below/above of each slab: every slab's upper neighbour has it as its
+    lower one (the halo written and the halo read are the same pair)."""
+    assert neighbours(0, 1, True) == (0, 0)
+    assert neighbours(0, 1, False) == (None, None)
+    assert neighbours(0, 2, True) == (1, 1)
+    assert [neighbours(r, 3, False) for r in range(3)] == [(None, 1), (0, 2), (1, None)]
+    for n in (1, 2, 3, 5):
+        for periodic in (False, True):
+            for r in range(n):
+                down, up = neighbours(r, n, periodic)
+                if up is not None:
+                    assert neighbours(up, n, periodic)[0] == r
+                if down is not None:
+                    assert neighbours(down, n, periodic)[1] == r
 
 
 def test_split_planes():
