@@ -159,7 +159,7 @@ __device__ __forceinline__ void cta_sum3(unsigned int& a, unsigned int& b, unsig
 // One fused pass (sweep.cuh FusedPhase) of a replica by its CTA group: the
 // group's CTAs walk the replica's units grid-stride with the plain kernels'
 // unit_step, so the chain is the one the replica follows alone.
-template <int PHASE, bool PERIODIC, int THREADS>
+template <int PHASE, bool PERIODIC, bool FULL, int THREADS>
 __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
                                            uint32_t step, float d, unsigned int& nacc,
                                            unsigned int& nflip) {
@@ -181,8 +181,9 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   const uint32_t per_colour = plane * (uint32_t)L.nk;
   for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units; g += stride) {
     if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-    unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, step, d, cp, key,
-                                                                   replica, nacc, nflip);
+    unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER, FULL>(L, G, g, step, d, cp,
+                                                                         key, replica, nacc,
+                                                                         nflip);
   }
 }
 
@@ -190,10 +191,15 @@ template <int PHASE, int THREADS>
 __device__ __forceinline__ void group_pass(const ReplicaDesc& D, int rank, int nct,
                                            uint32_t step, float d, unsigned int& nacc,
                                            unsigned int& nflip) {
-  if (D.L.periodic)
-    group_loop<PHASE, true, THREADS>(D, rank, nct, step, d, nacc, nflip);
-  else
-    group_loop<PHASE, false, THREADS>(D, rank, nct, step, d, nacc, nflip);
+  // a replica whose ni is a multiple of 4 has no padding slots
+  const bool full = D.L.ni % 4 == 0;
+  if (D.L.periodic) {
+    if (full) group_loop<PHASE, true, true, THREADS>(D, rank, nct, step, d, nacc, nflip);
+    else group_loop<PHASE, true, false, THREADS>(D, rank, nct, step, d, nacc, nflip);
+  } else {
+    if (full) group_loop<PHASE, false, true, THREADS>(D, rank, nct, step, d, nacc, nflip);
+    else group_loop<PHASE, false, false, THREADS>(D, rank, nct, step, d, nacc, nflip);
+  }
 }
 
 // FP64 moments of one replica's current state (moments.cuh), summed by its

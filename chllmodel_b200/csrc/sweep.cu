@@ -175,7 +175,7 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 // peer: the halo planes of neighbouring z-slabs that this slab's boundary
 // planes are written to (null pointers for a whole lattice).  The periodic
 // whole-lattice mode has no peers.
-template <int PHASE, int BMODE>
+template <int PHASE, int BMODE, bool FULL>
 __global__ void __launch_bounds__(kThreads, 2)
     fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, PhiloxKeys keys,
                       uint32_t replica, Control* __restrict__ ctl, PeerPlanes peer) {
@@ -194,14 +194,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
     for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
       if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
-                                                          replica, nacc, nflip);
+      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER, FULL>(L, G, g, (uint32_t)step, d, cp,
+                                                                keys, replica, nacc, nflip);
     }
   } else {
     for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
       if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, G, g, (uint32_t)step, d, cp, keys,
-                                                          replica, nacc, nflip, peer);
+      unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER, FULL>(L, G, g, (uint32_t)step, d, cp,
+                                                                keys, replica, nacc, nflip, peer);
     }
     // the halo stores reach the other GPU before this kernel counts as done
     __threadfence_system();
@@ -262,14 +262,15 @@ const StagedKernel kStaged[2][4] = {
 using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*,
                             PeerPlanes);
 
-// [boundary mode][phase]
-const FusedKernel kFused[3][4] = {
-    {fused_pass_kernel<kFusedA0, kBoundOpen>, fused_pass_kernel<kFusedA, kBoundOpen>,
-     fused_pass_kernel<kFusedB, kBoundOpen>, fused_pass_kernel<kFusedF, kBoundOpen>},
-    {fused_pass_kernel<kFusedA0, kBoundPeriodic>, fused_pass_kernel<kFusedA, kBoundPeriodic>,
-     fused_pass_kernel<kFusedB, kBoundPeriodic>, fused_pass_kernel<kFusedF, kBoundPeriodic>},
-    {fused_pass_kernel<kFusedA0, kBoundSlabXY>, fused_pass_kernel<kFusedA, kBoundSlabXY>,
-     fused_pass_kernel<kFusedB, kBoundSlabXY>, fused_pass_kernel<kFusedF, kBoundSlabXY>}};
+// [boundary mode][phase][ni a multiple of 4]
+#define CHLL_FUSED_ROW(M)                                                                       \
+  {{fused_pass_kernel<kFusedA0, M, false>, fused_pass_kernel<kFusedA0, M, true>},               \
+   {fused_pass_kernel<kFusedA, M, false>, fused_pass_kernel<kFusedA, M, true>},                 \
+   {fused_pass_kernel<kFusedB, M, false>, fused_pass_kernel<kFusedB, M, true>},                 \
+   {fused_pass_kernel<kFusedF, M, false>, fused_pass_kernel<kFusedF, M, true>}}
+const FusedKernel kFused[3][4][2] = {CHLL_FUSED_ROW(kBoundOpen), CHLL_FUSED_ROW(kBoundPeriodic),
+                                     CHLL_FUSED_ROW(kBoundSlabXY)};
+#undef CHLL_FUSED_ROW
 
 // Largest dynamic shared memory a staged CTA may ask for (2 stages).
 constexpr size_t kStagedSmemMax = 200 * 1024;
@@ -280,7 +281,7 @@ constexpr size_t kStagedSmemMax = 200 * 1024;
 struct DeviceShape {
   int sms = 0;
   int per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  int fused_per_sm[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+  int fused_per_sm[3][4][2] = {};
   size_t staged_smem[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last size asked per kernel
   int staged_per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
@@ -306,8 +307,10 @@ DeviceShape& device_shape() {
     for (int per = 0; per < 2; ++per)
       for (int p = 0; p < 4; ++p) {
         s.per_sm[per][p] = occupancy(kKernels[per][p]);
-        s.fused_per_sm[per][p] = occupancy(kFused[per][p]);
-        if (per == 1) s.fused_per_sm[2][p] = occupancy(kFused[2][p]);
+        for (int f = 0; f < 2; ++f) {
+          s.fused_per_sm[per][p][f] = occupancy(kFused[per][p][f]);
+          if (per == 1) s.fused_per_sm[2][p][f] = occupancy(kFused[2][p][f]);
+        }
         cudaFuncSetAttribute(kStaged[per][p], cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kStagedSmemMax);
       }
@@ -376,7 +379,8 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
   const int m = bmode < 0 ? 0 : (bmode > 2 ? 2 : bmode);
   const uint32_t n = G.units - G.first;
   const uint32_t need = (n + kThreads - 1) / kThreads;
-  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3];
+  const int full = L.ni % 4 == 0;
+  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3][full];
   const dim3 grid(need < resident ? (need ? need : 1) : resident);
   // The first and last planes of the unit range: slots 2*first .. and the
   // plane before slot 2*units.
@@ -386,8 +390,8 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
   peer.hi = m == kBoundPeriodic ? nullptr : peer_hi;
   peer.lo_first = 2 * G.first;
   peer.hi_first = 2 * G.units - peer.plane;
-  kFused[m][phase & 3]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1), replica,
-                                                       ctl, peer);
+  kFused[m][phase & 3][full]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1),
+                                                             replica, ctl, peer);
 }
 
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,

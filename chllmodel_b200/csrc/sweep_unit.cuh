@@ -130,7 +130,8 @@ struct UnitNbhd {
   bool fx0, fx1, fy, fz;
 };
 
-template <int C, bool PXY, bool PZ>
+// FULL: ni is a multiple of 4, so no unit holds a padding slot.
+template <int C, bool PXY, bool PZ, bool FULL = false>
 __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                             UnitNbhd& U) {
   const uint32_t hx = (uint32_t)L.hx;
@@ -146,8 +147,8 @@ __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeo
   const uint32_t o = (C + j + k) & 1u;
   const uint32_t i0 = 4 * q + o;
   const uint32_t i1 = i0 + 2;
-  U.v0 = i0 < ni;
-  U.v1 = i1 < ni;
+  U.v0 = FULL || i0 < ni;
+  U.v1 = FULL || i1 < ni;
   const uint32_t rs = row * hx;  // slot of the row start
   U.cen = L.col[C] + rs + 2 * q;
   const UnitSlots own = ld_unit(U.cen);
@@ -216,15 +217,15 @@ struct PeerPlanes {
 // Updates unit g in place with the trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.  A unit's slots are 2g (rows of hx = 2Q).
-template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY,
-          class PEER = NoPeer>
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
+          bool FULL = false, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica,
                                           unsigned int& nacc, unsigned int& nflip,
                                           const PEER& peer = PEER()) {
   UnitNbhd U;
-  gather_unit<C, PXY, PZ>(L, G, g, U);
+  gather_unit<C, PXY, PZ, FULL>(L, G, g, U);
   unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(U.n0, U.n1, U.nb0, U.nb1, U.v0, U.v1, g + G.goff,
                                                step, d, cp, key, replica, nacc, nflip);
   st_unit(U.cen, U.n0, U.n1);
