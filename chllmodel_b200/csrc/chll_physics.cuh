@@ -108,11 +108,22 @@ __device__ __forceinline__ float flip_dE(float c, float s, const Coupling& cp) {
   return __fmul_rn(s, fmaf(-cp.K, c, __fmul_rn(2.0f, cp.g)));
 }
 
+// 2^x by the hardware approximation (PTX ex2.approx, subnormals flushed).
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Metropolis rule of chll_mod.f90:188-200: accept if dE < 0, else if
-// u <= exp(-dE/kT).  At kT = 0 this gives exp(-inf) = 0 for dE > 0 and NaN
-// (reject) for dE = 0, as the reference's division does.
+// u <= exp(-dE/kT), evaluated as 2^(dE c) with c = -log2(e)/kT (the identity
+// exp(x) = 2^(x log2 e); c is the same for every trial of a launch, so the
+// compiler computes it once).  At kT = 0, c = -inf gives 2^-inf = 0 for
+// dE > 0 and NaN (reject) for dE = 0, as the reference's division does.
+// Flushing subnormals changes nothing: the smallest nonzero uniform is 2^-24.
 __device__ __forceinline__ bool metropolis(float dE, float u, float inv_kT) {
-  return (dE < 0.f) || (u <= __expf(__fmul_rn(-dE, inv_kT)));
+  const float c = __fmul_rn(-inv_kT, 1.4426950408889634f);  // -log2(e)/kT
+  return (dE < 0.f) || (u <= ex2_approx(__fmul_rn(dE, c)));
 }
 
 // Both sites of unit g of colour C (sites present: v0, v1), with the block's
