@@ -40,9 +40,9 @@ BATCH_NOUT = 50
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # DRAM read + write per site and launch of the fused pass kernels, measured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
-# B) on a 256^3 launch and scaled by sites to 480^3: 370.1 MB (A) and
-# 370.5 MB (B) per launch of 16.78 M sites.
-TRAFFIC_BYTES_PER_SITE_PASS = 22.07
+# B) on a 256^3 launch and scaled by sites to 480^3: 372.3 MB (A) and
+# 372.2 MB (B) per launch of 16.78 M sites.
+TRAFFIC_BYTES_PER_SITE_PASS = 22.19
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
@@ -372,8 +372,8 @@ def gpu_arm(args):
                      "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
                      "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
-                     "limiter": "instruction issue (ncu on 256^3: ~270 instructions per site, "
-                                "issue 64-65%, DRAM 42-43%, load waits hidden by an L1 prefetch); "
+                     "limiter": "instruction issue (ncu on 256^3: ~245 instructions per site, "
+                                "issue 65-66%, DRAM 46-47%, load waits hidden by an L1 prefetch); "
                                 "bytes are the algorithmic 24 B/site",
                      "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
                      "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,

