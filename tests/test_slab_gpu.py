@@ -153,3 +153,48 @@ def test_slab_peers_are_checked():
     assert rc == _lib.CHLL_EINVAL and b"not a slab" in L.chll_last_error()
     for x in (a, b, whole):
         x.close()
+
+
+def test_torch_peer_halo_with_one_nccl_rank():
+    """TorchPeerHalo on its NCCL path (the collectives ordered on the stream)
+    with a one-rank group: one periodic slab is its own neighbour, so its
+    passes store their boundary planes into their own halos, and it follows
+    the whole lattice's chain."""
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from chllmodel_b200.lattice import Lattice, coupling
+    from chllmodel_b200.slab import SlabLattice, TorchPeerHalo, sweep_slabs
+
+    shape = (12, 10, 8)
+    cp = coupling(0.7, 1.0, 0.1)
+    whole = Lattice(*shape, boundary="periodic")
+    whole.init_random(9)
+    whole.set_control(0.2, step=1)
+    whole.sweep(cp, 5, seed=3)
+    ref = whole.download_f4(), whole.control()
+    whole.close()
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1,
+                            device_id=torch.device("cuda", torch.cuda.current_device()))
+    try:
+        sl = SlabLattice(*shape, 0, shape[2], boundary="periodic")
+        sl.init_random(9)
+        sl.set_control(0.2, step=1)
+        halo = TorchPeerHalo.for_slab(sl)
+        sweep_slabs([sl], halo, cp, 2, seed=3)
+        sweep_slabs([sl], halo, cp, 3, seed=3)
+        torch.cuda.synchronize()
+        assert np.array_equal(sl.download_f4(), ref[0])
+        assert sl.control() == ref[1]
+        halo.close()
+        sl.close()
+    finally:
+        dist.destroy_process_group()
