@@ -291,7 +291,10 @@ int chll_lattice_control_update(chll_lattice* lat, int pass);
  * the count sums already give.  NULL = no such neighbour.  32-byte aligned
  * device addresses this GPU can store to: another slab's plane on this GPU
  * (chll_lattice_slab_plane) or a neighbouring GPU's, mapped with
- * chll_ipc_open.  Replaces the caller's halo copies (slab.py TorchHalo). */
+ * chll_ipc_open.  Replaces the caller's halo copies (slab.py TorchHalo).
+ * The addresses are used by every later pass: clear them (all NULL) before
+ * the memory they point to is freed or unmapped.  Waits for the lattice's
+ * stream before changing them. */
 int chll_lattice_slab_set_peers(chll_lattice* lat, void* lower0, void* lower1, void* upper0,
                                 void* upper1);
 /* Copies the first and last own planes of colour `colour` to the peers set
@@ -299,7 +302,8 @@ int chll_lattice_slab_set_peers(chll_lattice* lat, void* lower0, void* lower1, v
 int chll_lattice_slab_push(chll_lattice* lat, int colour);
 /* IPC export of the lattice's device allocation: the 64-byte
  * cudaIpcMemHandle_t into handle64 and the allocation's address in this
- * process (a plane's offset in it = its address - base). */
+ * process (a plane's offset in it = its address - base).  The exporting
+ * process must not destroy the lattice while another process has it mapped. */
 int chll_lattice_ipc_handle(chll_lattice* lat, void* handle64, uint64_t* base);
 /* Maps an allocation exported by another process (chll_lattice_ipc_handle)
  * into this one: *ptr = its base here.  chll_ipc_close unmaps it. */
