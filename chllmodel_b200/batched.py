@@ -142,6 +142,11 @@ class Batch:
         if wave_bytes is not None:
             check(self._L.chll_batch_set_wave_bytes(self._h, int(wave_bytes)))
 
+    def set_wait_limit(self, polls):
+        """Polls a replica group's barrier wait makes before it gives up and
+        sets the replica's status word (default 2^24)."""
+        check(self._L.chll_batch_set_wait_limit(self._h, int(polls)))
+
     def tuning(self) -> dict:
         t, c, w, n = ct.c_int32(), ct.c_int32(), ct.c_int64(), ct.c_int32()
         check(self._L.chll_batch_get_tuning(self._h, ct.byref(t), ct.byref(c), ct.byref(w),

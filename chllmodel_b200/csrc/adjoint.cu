@@ -25,7 +25,6 @@ namespace chll {
 namespace {
 
 constexpr int kGradThreads = 256;
-constexpr int kGradMaxBlocks = 148 * 4;
 
 // Slot t of colour `col` -> lattice site (i, j, k), with 32-bit divisions by
 // multiplication (a colour holds < 2^31 slots); false for a padding slot.
@@ -154,8 +153,9 @@ __device__ __forceinline__ void finish_sums(const double acc[4], double* __restr
   if (threadIdx.x == 0) *ticket = 0;
 }
 
-// One slot per thread: any alignment of the colour arrays (caller-provided
-// arrays of chll_energy_grad_noalloc).
+// One slot per thread: colour arrays that are 16-byte aligned but not 32
+// (caller-provided arrays of chll_energy_grad_noalloc; every slot is read as
+// one float4).
 __global__ void __launch_bounds__(kGradThreads)
     energy_grad_site_kernel(LatticeView L, MomentGeom M, CouplingD cd, float4* __restrict__ grad_rb,
                        int project,

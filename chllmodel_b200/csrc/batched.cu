@@ -437,7 +437,8 @@ struct chll_batch {
   cudaGraphExec_t graph = nullptr;
   int g_sweeps = -1, g_every = -1, g_from = -1, g_grid = -1, g_threads = -1;
   long long g_waves = -1;
-  unsigned long long limit = 1ull << 24;
+  unsigned long long limit = 1ull << 24;  // polls of a group-barrier wait before it gives up
+  unsigned long long g_limit = 0;
   long long total_sites = 0;
 
   chll::LatticeView view(int r) const { return desc[r].L; }
@@ -569,7 +570,8 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
   int rc = shape_launch(B);
   if (rc != CHLL_OK) return rc;
   if (!(B->graph && B->g_sweeps == nsweeps && B->g_every == every && B->g_from == from &&
-        B->g_grid == B->grid && B->g_threads == B->threads && B->g_waves == B->wave_bytes)) {
+        B->g_grid == B->grid && B->g_threads == B->threads && B->g_waves == B->wave_bytes &&
+        B->g_limit == B->limit)) {
     if (B->graph) cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
     cudaGraph_t g = nullptr;
@@ -587,6 +589,7 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
     B->g_grid = B->grid;
     B->g_threads = B->threads;
     B->g_waves = B->wave_bytes;
+    B->g_limit = B->limit;
   }
   BATCH_CUDA(cudaGraphLaunch(B->graph, B->stream));
   return CHLL_OK;
@@ -836,6 +839,12 @@ int chll_batch_info(chll_batch* B, int64_t* total_sites, int32_t* nreplicas, int
   if (nreplicas) *nreplicas = B->n;
   if (threads) *threads = B->threads;
   if (grid) *grid = B->grid;
+  return chll::record_ok();
+}
+
+int chll_batch_set_wait_limit(chll_batch* B, uint64_t polls) {
+  if (!B || polls == 0) return fail(CHLL_EINVAL, "batch_set_wait_limit: need a batch and polls >= 1");
+  B->limit = polls;
   return chll::record_ok();
 }
 

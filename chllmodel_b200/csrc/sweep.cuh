@@ -61,6 +61,10 @@ void launch_observables(const LatticeView& L, const MomentGeom& M, const Couplin
 void launch_energy_grad(const LatticeView& L, const CouplingD& cp, float4* grad_rb, int project,
                         double* partials, unsigned int* ticket, double* out4,
                         cudaStream_t stream);
+// The adjoint kernels run at most kGradMaxBlocks CTAs (grid-stride beyond
+// that), each leaving four FP64 partial sums: the partial-sum buffers of the
+// adjoint hold kGradMaxBlocks * 4 doubles on any GPU.
+constexpr int kGradMaxBlocks = 148 * 4;
 int energy_grad_max_blocks();
 // adjoint.cu: one colour of the zero-temperature gradient quench.
 void launch_quench_pass(const LatticeView& L, const CouplingD& cd, float eta, int colour,

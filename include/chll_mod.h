@@ -250,6 +250,14 @@ int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
  * (0, the default: all replicas in one wave), largest first; each wave gets
  * the whole co-resident grid, in the same launch. */
 int chll_batch_set_wave_bytes(chll_batch* b, int64_t wave_bytes);
+/* How many polls a replica group's barrier wait makes before it gives up
+ * (default 2^24, seconds of waiting; >= 1).  A wait that gives up sets the
+ * replica's status word (column 15 of its chll_batch_moments row); every CTA
+ * of that replica then leaves the launch at its next barrier, the other
+ * replicas run on, and chll_batch_moments returns CHLL_EDEVICE.  The
+ * replica's state after such a launch is not usable.  No counterpart in the
+ * reference, which has no batched launch. */
+int chll_batch_set_wait_limit(chll_batch* b, uint64_t polls);
 int chll_batch_get_tuning(chll_batch* b, int32_t* threads, int32_t* ctas_per_sm,
                           int64_t* wave_bytes, int32_t* nwaves);
 /* Times every launch shape (threads, CTAs per SM, wave size) for trial_sweeps
@@ -345,9 +353,13 @@ int chll_lattice_projection(chll_lattice* lat, const int* plane, long long* hist
  * All intermediates live in one fixed device array of this library (about
  * 4 MiB on every GPU that loads it, held until exit): lattices needing more
  * than 262,144 red/black slots (2*hx*nj*nk; a 64^3 lattice fits) are rejected
- * with CHLL_ERANGE.  The first call on each device looks up that array's
- * device address; make it before any stream capture.  Calls share the array:
- * calls whose work overlaps on the GPU race and must be serialised. */
+ * with CHLL_ERANGE.  colour0, colour1 and grad must be 16-byte aligned and
+ * out4 8-byte aligned, all on the current device (or managed), else
+ * CHLL_EINVAL before anything is enqueued.  The first call on each device
+ * looks up that array's device address; make it before any stream capture
+ * (calls outside a capture look it up again, so a device reset leaves no
+ * stale address).  Calls share the array: calls whose work overlaps on the
+ * GPU race and must be serialised. */
 int chll_energy_grad_noalloc(const void* colour0, const void* colour1, int ni, int nj, int nk,
                              int boundary, const chll_coupling* c, int project, float* grad,
                              double* out4, void* stream);

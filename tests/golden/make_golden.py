@@ -1,7 +1,8 @@
 """Generates the committed golden fixtures under tests/golden/.
 
-Run in a checkout that has the reference tree at /root/reference
-(``python tests/golden/make_golden.py``); the fixtures it writes are small
+Run with the path of a mdeutsc2/ChLLModel checkout
+(``python tests/golden/make_golden.py --reference PATH``, or the
+environment variable CHLL_REFERENCE_TREE); the fixtures it writes are small
 and committed, and nothing at test time reads the reference tree.
 
 1. ``ekernel_energy.npz`` -- the reference's own independent restatement of
@@ -31,7 +32,7 @@ import textwrap
 
 import numpy as np
 
-REF = "/root/reference"
+REF = os.environ.get("CHLL_REFERENCE_TREE", "")  # set by main() from --reference
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -155,6 +156,15 @@ def make_analysis_fixture(path):
 
 
 def main():
+    global REF
+    import argparse
+
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=REF,
+                    help="path of a mdeutsc2/ChLLModel checkout (or CHLL_REFERENCE_TREE)")
+    REF = ap.parse_args().reference
+    if not REF or not os.path.isdir(os.path.join(REF, "notebooks")):
+        ap.error("give --reference PATH (or CHLL_REFERENCE_TREE): a ChLLModel checkout")
     make_ekernel_fixture(os.path.join(HERE, "ekernel_energy.npz"))
     make_analysis_fixture(os.path.join(HERE, "analysis_golden.npz"))
     with open(os.path.join(HERE, "philox_kat.json"), "w") as f:

@@ -130,3 +130,39 @@ def test_batch_rejects_bad_specs():
         Batch([replica(7, kT=1.0, K=1.0, boundary="periodic")])
     with pytest.raises(_lib.ChllError, match="kT"):
         Batch([replica(8, kT=-1.0, K=1.0)])
+
+
+def test_batch_barrier_wait_gives_up():
+    """A group-barrier wait limited to one poll runs out on a replica of many
+    CTAs: its status word is set, its CTAs leave the launch, the one-CTA
+    replica (which never waits) finishes every sweep, chll_batch_moments
+    reports CHLL_EDEVICE, and the context stays usable."""
+    import ctypes as ct
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.batched import Batch, replica
+
+    L = _lib.load()
+    nsw = 40
+    specs = [replica(64, kT=0.5, K=1.0, seed=3, replica=0),
+             replica(8, kT=0.5, K=1.0, seed=4, replica=1)]
+    with Batch(specs) as b:
+        b.set_tuning(128, 0)
+        assert b.info()["grid"] > 2  # the 64^3 replica spans many CTAs
+        b.init_random()
+        b.set_wait_limit(1)
+        b.run(nsw, measure_every=10)
+        m = np.zeros((2, 16), np.float64)
+        rc = L.chll_batch_moments(b._h, m.ctypes.data_as(ct.c_void_p))
+        assert rc == _lib.CHLL_EDEVICE
+        assert "timed out" in _lib.last_error()
+        assert m[0, 15] != 0
+        assert m[1, 15] == 0 and int(m[1, 12]) == nsw + 1
+    with pytest.raises(_lib.ChllError):
+        Batch(specs).set_wait_limit(0)
+    # a new batch with the default limit runs cleanly on the same context
+    with Batch(specs) as b:
+        b.init_random()
+        b.run(4, measure_every=2)
+        m = b.moments()
+        assert np.all(m[:, 15] == 0) and np.all(m[:, 12] == 5)

@@ -110,6 +110,44 @@ def test_noalloc_adjoint_on_16_byte_aligned_arrays():
     lat.close()
 
 
+def test_noalloc_adjoint_refuses_misaligned_arrays():
+    """Arrays that are not float4 (16-byte) aligned, or an out4 that is not
+    8-byte aligned, are refused on the host before any launch: a kernel
+    given them would fault on its vector accesses and lose the context."""
+    import torch
+
+    from chllmodel_b200 import _lib
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    L = _lib.load()
+    shape = (16, 12, 8)
+    lat = Lattice(*shape, boundary="periodic")
+    lat.init_random(seed=2)
+    c0, c1, _, _ = lat.storage()
+    n = lat.nsites
+    buf = torch.zeros(4 * n + 8, dtype=torch.float32, device="cuda")
+    out = torch.zeros(8, dtype=torch.float64, device="cuda")
+    grad = buf.data_ptr()
+    out4 = out.data_ptr()
+    cp = coupling(0.3, 1.0)
+    args = dict(c0=c0, c1=c1, grad=grad, out4=out4)
+    for key, off in (("c0", 8), ("c1", 4), ("grad", 8), ("out4", 4)):
+        a = dict(args)
+        a[key] += off
+        rc = L.chll_energy_grad_noalloc(ct.c_void_p(a["c0"]), ct.c_void_p(a["c1"]), *shape,
+                                        _lib.CHLL_PERIODIC, ct.byref(cp), 1,
+                                        ct.c_void_p(a["grad"]), ct.c_void_p(a["out4"]), None)
+        assert rc == _lib.CHLL_EINVAL, key
+        assert "aligned" in _lib.last_error()
+    # the same call with aligned arrays runs
+    rc = L.chll_energy_grad_noalloc(ct.c_void_p(c0), ct.c_void_p(c1), *shape, _lib.CHLL_PERIODIC,
+                                    ct.byref(cp), 1, ct.c_void_p(grad), ct.c_void_p(out4), None)
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    assert torch.isfinite(out[:4]).all()
+    lat.close()
+
+
 class _DeviceF4:
     """(count, 4) float32 device array at an address, for torch.as_tensor."""
 
