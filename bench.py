@@ -7,12 +7,22 @@ chirality flips on both colours, run as the library's two fused passes):
   reference's adaptation, FP64 observables every 100 sweeps.  The float4
   lattice is 1.77 GB, far above the 126 MB L2, so no L2 flush is needed.
 
-Arms:
-  default            the CUDA library (one process per GPU, independent
-                     replicas, no collective on the data path: weak scaling)
-  --impl reference   the reference algorithm on the host cores (the C oracle
-                     port, OpenMP), each step one sweep of a bounded slab of
-                     the same lattice; rank 0 only.
+The line also carries, under "configs", the other benchmark configurations
+of the path, each timed on the GPU through the public API and on the host
+cores through the oracle port: the 32^3 reference-size run, the 128^3
+anneal, the 64^3 differentiation workflow and the batched 64-replica
+phase grid against the same points run one after another.
+
+Modes and arms:
+  default            the CUDA library, one 480^3 replica per GPU (seed 11 +
+                     rank), no collective on the data path: weak scaling
+  --mode slab        ONE lattice split into z-slabs, one per rank; each
+                     pass stores its boundary planes into the neighbours'
+                     halos over peer memory (CUDA IPC) and the per-pass
+                     accept counts are summed with NCCL: strong scaling
+  --impl reference   the reference algorithm on the host cores (the C
+                     oracle port, OpenMP over each colour), each step one
+                     sweep of the same 480^3 lattice; rank 0 only.
 
 Prints ONE JSON line (rank 0).
 """
@@ -23,6 +33,7 @@ import json
 import os
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -38,11 +49,12 @@ E2E_SWEEPS = 10000  # the 480^3 workload's run length (observables every NOUT sw
 # (scripts/phase_diagram.py:30, sim.run(200000, 50)).
 BATCH_NOUT = 50
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
-# DRAM read + write per site and launch of the fused pass kernels, measured
-# with ncu (dram__bytes_read.sum + dram__bytes_write.sum, mean of passes A and
-# B) on a 256^3 launch and scaled by sites to 480^3: 372.3 MB (A) and
-# 372.2 MB (B) per launch of 16.78 M sites.
-TRAFFIC_BYTES_PER_SITE_PASS = 22.19
+# ncu figures of the fused pass kernels A and B on the 480^3 benchmark lattice
+# (one capture of two launches, mean of A and B; profiles/fused_pass_kernel_480cube_metrics.md):
+# DRAM bytes read + written per site and launch, and warp-level instructions
+# x 32 per updated site (a launch updates half of the sites).
+PASS_PROFILE = {"traffic_bytes_per_site": 22.19, "thread_instr_per_updated_site": 245.0,
+                "source": "ncu on 256^3, scaled by sites"}
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
 WORKLOAD = (f"plain {L_EDGE}^3 periodic checkerboard sweep (director + chirality Metropolis), "
@@ -58,121 +70,198 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+# ---------------------------------------------------------------------------
+# Clock record of a timed region
+# ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event reasons while a region runs.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is polled from a thread every `period` seconds (2 ms: a 20-sweep
+    region of the 480^3 workload lasts ~25 ms), plus one sample on entry and
+    one on exit; without NVML, nvidia-smi -lms 100 is the fallback.  The GPU
+    is found by its PCI bus id, which NVML and CUDA share whatever
+    CUDA_VISIBLE_DEVICES says."""
 
-    _count = 0
+    REASON_BITS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+    SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    SMI_REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        ClockSampler._count += 1  # one file per sampler: several may be summarised late
-        self.path = os.path.join("/tmp", f"chll_clocks_{os.getpid()}_{ClockSampler._count}.csv")
+    def __init__(self, device: int, period: float = 0.002):
+        self.device = device
+        self.period = period
+        self.samples: list[tuple[float, int]] = []  # (sm MHz, reason bits)
+        self.sm_max = None
+        self.source = None
+        self._nvml = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._smi = None
+        self._smi_path = None
         self._summary = None
 
-    def __enter__(self):
+    def _bus_id(self):
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=self.fh, stderr=subprocess.DEVNULL)
-        except Exception:  # noqa: BLE001 - no nvidia-smi
-            self.proc = None
+            import torch
+
+            p = torch.cuda.get_device_properties(self.device)
+            return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:  # noqa: BLE001
+            return None
+
+    def _sample(self):
+        n, h = self._nvml, self._handle
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        reasons = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((float(sm), int(reasons)))
+
+    def _poll(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:  # noqa: BLE001
+                return
+            time.sleep(self.period)
+
+    def __enter__(self):
+        bus = self._bus_id()
+        try:
+            import pynvml as n
+
+            n.nvmlInit()
+            self._nvml = n
+            self._handle = (n.nvmlDeviceGetHandleByPciBusId(bus) if bus
+                            else n.nvmlDeviceGetHandleByIndex(self.device))
+            self.sm_max = float(n.nvmlDeviceGetMaxClockInfo(self._handle, n.NVML_CLOCK_SM))
+            self.source = "nvml"
+            self._sample()
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+        except Exception:  # noqa: BLE001 - no NVML: nvidia-smi, then nothing
+            self._nvml = None
+            self._start_smi(bus)
         return self
 
+    def _start_smi(self, bus):
+        ClockSampler._count = getattr(ClockSampler, "_count", 0) + 1
+        self._smi_path = os.path.join("/tmp", f"chll_clocks_{os.getpid()}_{ClockSampler._count}.csv")
+        try:
+            self._fh = open(self._smi_path, "w")
+            self._smi = subprocess.Popen(
+                ["nvidia-smi", f"--id={bus or self.device}", f"--query-gpu={self.SMI_FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self._fh, stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi"
+        except Exception:  # noqa: BLE001
+            self._smi = None
+
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        if self._nvml is not None:
+            self._stop.set()
+            if self._thread is not None:
+                self._thread.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
+                self._sample()
+                self._nvml.nvmlShutdown()
             except Exception:  # noqa: BLE001
-                self.proc.kill()
-        if getattr(self, "fh", None):
-            self.fh.close()
+                pass
+        if self._smi is not None:
+            self._smi.terminate()
+            try:
+                self._smi.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self._smi.kill()
+            self._fh.close()
 
-    def summary(self):
-        if self._summary is None:
-            self._summary = self._read()
-        return self._summary
-
-    def _read(self):
-        if self.proc is None or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+    @classmethod
+    def parse_smi_csv(cls, path):
+        """(samples [(sm MHz, reason bits)], max SM MHz) of an nvidia-smi CSV."""
+        samples, smax = [], None
+        for line in open(path):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
+                sm = float(parts[1])
                 smax = float(parts[2])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            bits = 0
+            for name, v in zip(cls.SMI_REASONS, parts[5:9]):
                 if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                    bits |= cls.REASON_BITS[name]
+            samples.append((sm, bits))
+        return samples, smax
+
+    def summary(self):
+        if self._summary is None:
+            if self._smi_path and os.path.exists(self._smi_path):
+                self.samples, self.sm_max = self.parse_smi_csv(self._smi_path)
+                os.unlink(self._smi_path)
+            if not self.samples:
+                self._summary = {"sm_mhz": None, "sm_max_mhz": self.sm_max, "reasons": [],
+                                 "samples": 0, "source": self.source or "unavailable"}
+            else:
+                sm = sorted(s for s, _ in self.samples)
+                bits = 0
+                for _, b in self.samples:
+                    bits |= b
+                self._summary = {
+                    "sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.sm_max,
+                    "reasons": sorted(n for n, m in self.REASON_BITS.items() if bits & m),
+                    "samples": len(sm), "source": self.source}
+        return self._summary
 
 
 # ---------------------------------------------------------------------------
 # CPU arm: the oracle port of the reference algorithm on the host cores
 # ---------------------------------------------------------------------------
-def cpu_sample(seconds: float, threads: int | None = None, nz: int = 8):
-    """Times reference sweeps of a 480 x 480 x nz periodic slab of the workload
-    on the host cores until `seconds` have elapsed (at least one sweep)."""
+def _oracle_lattice(edge, seed=SEED):
     from oracle import oracle as O
 
-    if threads:
-        O.set_threads(threads)
-    cores = O.max_threads()
-    cfg = O.make_cfg(L_EDGE, L_EDGE, nz, periodic=True, kT=KT, K=KK, g=FIELD, eps=EPS,
-                     seed=SEED)
-    nx, ny, nz_, s = O.init_random(cfg)
-    n = L_EDGE * L_EDGE * nz
+    cfg = O.make_cfg(edge, edge, edge, periodic=True, kT=KT, K=KK, g=FIELD, eps=EPS, seed=seed)
+    return O, cfg, O.init_random(cfg)
+
+
+def cpu_sample(seconds: float, edge: int = L_EDGE):
+    """Reference sweeps of the workload's edge^3 periodic lattice on the host
+    cores until `seconds` have elapsed (at least one sweep)."""
+    O, cfg, (nx, ny, nz, s) = _oracle_lattice(edge)
+    n = edge ** 3
     sweeps, t0, step = 0, time.perf_counter(), 1
     while True:
         for p in range(4):
-            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+            O.run_pass(cfg, p, step, D0, nx, ny, nz, s)
         step += 1
         sweeps += 1
         dt = time.perf_counter() - t0
         if dt >= seconds:
             break
-    return {"value": n * sweeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{sweeps} sweep(s) of a {L_EDGE}x{L_EDGE}x{nz} periodic slab "
-                      f"({n} sites) of the workload, {dt:.1f} s, FP64 reference arithmetic"}
+    return {"value": n * sweeps / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+            "sample": f"{sweeps} sweep(s) of the workload's {edge}^3 periodic lattice "
+                      f"({n} sites), {dt:.1f} s, FP64 reference arithmetic"}
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import oracle as O
-
+    edge = args.edge
+    O, cfg, (nx, ny, nz, s) = _oracle_lattice(edge)
     cores = O.max_threads()
-    nz = 8
-    cfg = O.make_cfg(L_EDGE, L_EDGE, nz, periodic=True, kT=KT, K=KK, g=FIELD, eps=EPS, seed=SEED)
-    nx, ny, nz_, s = O.init_random(cfg)
-    n = L_EDGE * L_EDGE * nz
+    n = edge ** 3
     step = 1
     for _ in range(args.warmup):
         for p in range(4):
-            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+            O.run_pass(cfg, p, step, D0, nx, ny, nz, s)
         step += 1
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         for p in range(4):
-            O.run_pass(cfg, p, step, D0, nx, ny, nz_, s)
+            O.run_pass(cfg, p, step, D0, nx, ny, nz, s)
         times.append(time.perf_counter() - t0)
         step += 1
     tot = sum(times)
@@ -182,11 +271,11 @@ def reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": [L_EDGE, L_EDGE, L_EDGE],
-                   "sample": f"each step one sweep of a {L_EDGE}x{L_EDGE}x{nz} periodic slab"},
+        "config": {"workload": _workload(edge), "lattice": [edge, edge, edge],
+                   "sample": f"each step one sweep of the whole {edge}^3 periodic lattice"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} sweeps of a {L_EDGE}x{L_EDGE}x{nz} periodic "
-                                   f"slab ({n} sites); the reference's Fortran/OpenACC build "
+                         "sample": f"{args.steps} sweeps of the {edge}^3 periodic lattice "
+                                   f"({n} sites); the reference's Fortran/OpenACC build "
                                    f"needs nvfortran, absent here, so its C restatement runs"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -194,9 +283,26 @@ def reference_arm(args):
     return 0
 
 
+def _workload(edge):
+    return WORKLOAD if edge == L_EDGE else WORKLOAD.replace(f"{L_EDGE}^3", f"{edge}^3")
+
+
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def _dist_init(torch, local):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    return dist
+
+
 def gpu_arm(args):
     import numpy as np
     import torch
@@ -205,14 +311,7 @@ def gpu_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = _dist_init(torch, local)
 
     def barrier():
         if dist is not None:
@@ -305,6 +404,7 @@ def gpu_arm(args):
         else np.zeros((0, 16))
     lat.close()
     del lat
+    clk = clocks.summary()
 
     # e2e: the public API with host buffers (pinned), copies inside the timed region
     e2e = None
@@ -323,7 +423,7 @@ def gpu_arm(args):
         nsw = max(args.e2e_sweeps, NOUT)
         sim.run(NOUT, NOUT)  # warm-up: allocations and graph capture
         barrier()
-        with ClockSampler(local) as e2e_clocks:
+        with ClockSampler(local, period=0.05) as e2e_clocks:
             t0 = time.perf_counter()
             sim.run(nsw, NOUT)
             dt = time.perf_counter() - t0
@@ -340,56 +440,210 @@ def gpu_arm(args):
                                      "download",
                "clocks": e2e_clocks.summary()}
 
-    batched = None
+    configs = {}
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = other_configs(args, torch)
     if not args.no_batched:
-        batched = batched_vs_plain(args, rank, torch)
+        configs["batched_64_replicas"] = batched_vs_plain(args, rank, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(args.cpu_seconds)
+        cpu = cpu_sample(args.cpu_seconds, edge)
 
-    clk = clocks.summary()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    # Issue roofline: every SM issues at most one warp instruction per cycle
+    # and scheduler (4 per SM), so a pass updating n/2 sites at I thread
+    # instructions each can update at most SMs * 4 * 32 * f / I sites per second.
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    instr = PASS_PROFILE["thread_instr_per_updated_site"]
+    f_hz = (clk["sm_mhz"] or clk["sm_max_mhz"] or 1965.0) * 1e6
+    issue_ceiling = sms * 4 * 32 * f_hz / instr
+    updated_per_s = (n / 2) / (pass_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: directors uniform on the sphere, chiralities +-1 p=1/2 "
                 "(Philox seed 11 + rank); state FP32, observables FP64",
-        "config": {"workload": WORKLOAD if edge == L_EDGE else WORKLOAD.replace(
-                       f"{L_EDGE}^3", f"{edge}^3"), "lattice": [edge, edge, edge],
+        "config": {"workload": _workload(edge), "lattice": [edge, edge, edge],
                    "boundary": "periodic", "kT": KT, "K": KK, "h": FIELD, "eps": EPS,
                    "d0": D0, "nout": NOUT, "parallelism": f"replicas x{world}",
                    "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak,
-                     "traffic": (TRAFFIC_BYTES_PER_SITE_PASS * n / 1e9
-                                 if TRAFFIC_BYTES_PER_SITE_PASS else None),
-                     "traffic_unit": "GB per launch (ncu, 256^3 launch scaled by sites)",
+                     "traffic": PASS_PROFILE["traffic_bytes_per_site"] * n / 1e9,
+                     "traffic_unit": f"GB per launch ({PASS_PROFILE['source']})",
                      "kernel": "fused_pass_kernel A and B (2 launches per step)",
                      "bytes_per_launch": BYTES_PER_SITE_PASS * n,
-                     "limiter": "instruction issue (ncu on 256^3: ~245 instructions per site, "
-                                "issue 65-66%, DRAM 46-47%, load waits hidden by an L1 prefetch); "
-                                "bytes are the algorithmic 24 B/site",
                      "ms_per_launch": pass_ms, "ms_pass_a": a_ms / args.steps,
                      "ms_pass_b": b_ms / args.steps, "peak_kind": peak_kind,
-                     "four_half_sweep_equiv_gbs": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)
-                     * args.steps / 1e9},
+                     "instructions_per_site": instr,
+                     "issue_frac": updated_per_s / issue_ceiling,
+                     "issue_note": "updated sites/s over SMs x 4 schedulers x 32 lanes x "
+                                   "median sampled SM clock / thread instructions per updated "
+                                   "site: the limiter of these passes"},
+        "reference_form": {
+            "note": "the reference's four half-sweeps move 96 B per site and sweep; the fused "
+                    "form does the same trials in two passes of 24 B per site",
+            "equiv_gbs_at_96_B_per_site_sweep": 4 * BYTES_PER_SITE_PASS * n / (ms * 1e-3)
+            * args.steps / 1e9},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk,
-        "batched": batched,
+        "configs": configs,
         "final_control": ctl,
         "last_row": {"energy_per_site": float(rows[-1][5] / n) if len(rows) else None,
                      "eta": float(rows[-1][1]) if len(rows) else None},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _events(torch, stream):
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    return a, b
+
+
+def other_configs(args, torch):
+    """The path's other benchmark configurations, each on the GPU through the
+    public API and on the host cores through the oracle port."""
+    import numpy as np
+
+    from chllmodel_b200 import chll
+    from chllmodel_b200.lattice import Lattice, coupling
+    from chllmodel_b200.workflows import anneal, linear_schedule
+    from oracle import oracle as O
+
+    out = {}
+    cores = O.max_threads()
+
+    # 32^3, K=0.5, h=0, kT=0.5, seed 1, 1000 sweeps with a row every 100:
+    # ChLLSim.run through chll_run_ex, host arrays, wall time of the call.
+    e = 32
+    lat = Lattice(e, e, e, boundary="periodic")
+    lat.init_random(1)
+    state = lat.download_f64()
+    lat.close()
+    sim = chll.ChLLSim(e, e, e, 0.5, 0.1, 0.5, 0.0, 0.0, seed=1, boundary="periodic",
+                       verbose=False)
+    runs = []
+    for r in range(4):  # the first call captures the graph
+        sim.nx[...], sim.ny[...], sim.nz[...], sim.s[...] = state
+        sim.d = 0.1
+        runs.append(sim.run(1000, 100))
+    t_gpu = float(np.median(runs[1:]))
+    cfg = O.make_cfg(e, e, e, periodic=True, kT=0.5, K=0.5, g=0.0, seed=1)
+    ox, oy, oz, os_ = (np.asfortranarray(a) for a in state)
+    t0 = time.perf_counter()
+    O.run(cfg, 1, 1000, 100, 0.1, ox, oy, oz, os_)
+    t_cpu = time.perf_counter() - t0
+    out["plain_32"] = {
+        "workload": "32^3 periodic, K=0.5, h=0, kT=0.5, d0=0.1, seed 1, 1000 sweeps, a "
+                    "measurement row every 100 (ChLLSim.run, host FP64 arrays)",
+        "seconds": t_gpu, "site_updates_per_s": e ** 3 * 1000 / t_gpu,
+        "cpu_seconds": t_cpu, "cpu_site_updates_per_s": e ** 3 * 1000 / t_cpu,
+        "cpu_cores": cores, "speedup_vs_cpu": t_cpu / t_gpu,
+        "final_d": sim.d, "final_row": [float(x) for x in sim.m[-1]]}
+
+    # 128^3 anneal: K=1, h=0.25, seed 7, kT 1.5 -> 0.1 in 20 stages of 500
+    # sweeps, FP64 rows every 10 sweeps (workflows.anneal).
+    e = 128
+    lat = Lattice(e, e, e, boundary="periodic")
+    sched = linear_schedule(1.5, 0.1, 20)
+    for rep in range(2):  # the first pass captures the graphs
+        lat.init_random(7)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        stages = anneal(lat, sched if rep else sched[:1], 500, K=1.0, g=0.25, seed=7,
+                        measure_every=10, d0=0.1)
+        lat.sync()
+        t_gpu = time.perf_counter() - t0
+    lat.close()
+    cfg = O.make_cfg(e, e, e, periodic=True, kT=1.5, K=1.0, g=0.25, seed=7)
+    ox, oy, oz, os_ = O.init_random(cfg)
+    ncpu = 60
+    t0 = time.perf_counter()
+    for st in range(1, ncpu + 1):
+        for p in range(4):
+            O.run_pass(cfg, p, st, 0.1, ox, oy, oz, os_)
+    t_cpu = (time.perf_counter() - t0) * 10000 / ncpu
+    out["anneal_128"] = {
+        "workload": "128^3 periodic, K=1, h=0.25, seed 7, kT 1.5 -> 0.1 linear in 20 stages of "
+                    "500 sweeps, FP64 rows every 10 sweeps (workflows.anneal)",
+        "seconds": t_gpu, "site_updates_per_s": e ** 3 * 10000 / t_gpu,
+        "cpu_seconds_extrapolated": t_cpu, "cpu_sample": f"{ncpu} sweeps at kT=1.5, scaled to "
+                                                          f"10000", "cpu_cores": cores,
+        "speedup_vs_cpu": t_cpu / t_gpu,
+        "last_stage": {k: stages[-1][k] for k in ("kT", "energy", "eta", "S", "C_v", "chi_c")}}
+
+    # 64^3 differentiation: 500-sweep equilibration at kT=0.3, K=1, h=0.5
+    # (seed 3), the energy adjoint (dE/dn and dE/d(eps, K, h)), a 2000-step
+    # zero-temperature gradient quench.
+    e = 64
+    stream = torch.cuda.current_stream()
+    lat = Lattice(e, e, e, boundary="periodic")
+    lat.set_stream(stream.cuda_stream)
+    lat.init_random(3)
+    lat.set_control(0.1, step=1)
+    cpe = coupling(0.3, 1.0, 0.5)
+    lat.sweep(cpe, 10, seed=3)  # graph capture
+    lat.init_random(3)
+    lat.set_control(0.1, step=1)
+    a, b = _events(torch, stream)
+    a.record(stream)
+    lat.sweep(cpe, 500, seed=3)
+    b.record(stream)
+    b.synchronize()
+    t_eq = a.elapsed_time(b) * 1e-3
+    grad = torch.empty((e ** 3, 4), dtype=torch.float32, device="cuda")
+    cpq = coupling(0.0, 1.0, 0.5)
+    lat.energy_grad(cpq, project=True, grad_ptr=grad.data_ptr())  # allocation
+    reps = 20
+    a.record(stream)
+    for _ in range(reps):
+        _, out4 = lat.energy_grad(cpq, project=True, grad_ptr=grad.data_ptr())
+    b.record(stream)
+    b.synchronize()
+    t_adj = a.elapsed_time(b) * 1e-3 / reps
+    x, y, z, s = lat.download_f64()
+    e_before = float(out4[0])
+    lat.quench(cpq, 0.05, 2)
+    lat.sync()
+    a.record(stream)
+    lat.quench(cpq, 0.05, 2000)
+    b.record(stream)
+    b.synchronize()
+    t_q = a.elapsed_time(b) * 1e-3
+    _, out4q = lat.energy_grad(cpq)
+    lat.close()
+    cfg = O.make_cfg(e, e, e, periodic=True, kT=0.0, K=1.0, g=0.5, seed=3)
+    ox, oy, oz, os_ = (np.asfortranarray(v) for v in (x, y, z, s))
+    t0 = time.perf_counter()
+    O.energy_grad(cfg, ox, oy, oz, os_, project=True)
+    t_cadj = time.perf_counter() - t0
+    cfg = O.make_cfg(e, e, e, periodic=True, kT=0.3, K=1.0, g=0.5, seed=3)
+    t0 = time.perf_counter()
+    for st in range(1, 51):
+        for p in range(4):
+            O.run_pass(cfg, p, st, 0.1, ox, oy, oz, os_)
+    t_ceq = (time.perf_counter() - t0) * 10
+    out["differentiation_64"] = {
+        "workload": "64^3 periodic, 500-sweep equilibration at kT=0.3, K=1, h=0.5 (seed 3); "
+                    "energy adjoint (tangent-projected dE/dn, dE/d(eps,K,h)); 2000-step "
+                    "gradient quench at kT=0, step 0.05",
+        "equilibration_seconds": t_eq, "equilibration_site_updates_per_s": e ** 3 * 500 / t_eq,
+        "adjoint_ms": t_adj * 1e3, "quench_seconds": t_q,
+        "quench_site_steps_per_s": e ** 3 * 2000 / t_q,
+        "energy_before_quench": e_before, "energy_after_quench": float(out4q[0]),
+        "cpu_adjoint_ms": t_cadj * 1e3, "cpu_equilibration_seconds_extrapolated": t_ceq,
+        "cpu_cores": cores}
+    return out
 
 
 def batched_vs_plain(args, rank, torch):
@@ -493,16 +747,108 @@ def batched_vs_plain(args, rank, torch):
             "mean_S_highest_kT": float(np.mean([r["S"] for r in summ if r["kT"] > 1.9]))}
 
 
+# ---------------------------------------------------------------------------
+# Slab mode: one lattice split over the ranks
+# ---------------------------------------------------------------------------
+def slab_arm(args):
+    """One edge^3 periodic lattice in z-slabs, one per rank.  Every pass
+    stores the slab's boundary planes into the neighbours' halo planes over
+    peer memory (CUDA IPC mappings; a single rank is its own neighbour) and
+    the per-pass counts are summed with NCCL, which also orders the passes
+    across ranks.  Timed: the sweeps with their closing flip pass, halo
+    stores and count all-reduces, on the device (CUDA events), max over ranks."""
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world == 1:  # a one-rank group: the slab's halos are its own planes
+        import socket
+
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            os.environ.setdefault("MASTER_PORT", str(s.getsockname()[1]))
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    from chllmodel_b200.lattice import coupling
+    from chllmodel_b200.slab import SlabLattice, TorchPeerHalo, split_planes, sweep_slabs
+
+    edge = args.edge
+    n = edge ** 3
+    z0, nkl = split_planes(edge, world)[rank]
+    cp = coupling(KT, KK, FIELD, EPS)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        sl = SlabLattice(edge, edge, edge, z0, nkl, boundary="periodic")
+        sl.init_random(SEED)
+        sl.set_control(D0, step=1)
+        halo = TorchPeerHalo.for_slab(sl)
+        sweep_slabs([sl], halo, cp, args.warmup, seed=SEED)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            e0.record(stream)
+            sweep_slabs([sl], halo, cp, args.steps, seed=SEED)
+            e1.record(stream)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ctl = sl.control()
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+        halo.close()
+        sl.close()
+    torch.cuda.synchronize()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": n * args.steps / (ms * 1e-3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: directors uniform on the sphere, chiralities +-1 p=1/2 (Philox "
+                "seed 11); state FP32",
+        "config": {"workload": f"one {edge}^3 periodic lattice in {world} z-slab(s), the "
+                               f"{_workload(edge)} minus its measurements",
+                   "mode": "slab", "lattice": [edge, edge, edge],
+                   "slab_planes": [list(p) for p in split_planes(edge, world)],
+                   "transport": "boundary planes stored into the neighbours' halos by the "
+                                "passes (CUDA IPC peer memory), counts summed with NCCL",
+                   "parallelism": f"z-slabs x{world}",
+                   "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
+        "e2e": None, "e2e_note": "slab mode times device-resident sweeps only",
+        "gpu_launches": None, "clocks": clocks.summary(), "final_control": ctl,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "slab"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-sweeps", type=int, default=E2E_SWEEPS,
                     help="sweeps of the end-to-end ChLLSim.run (default: the workload's 10000)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 32^3, 128^3 anneal and 64^3 differentiation configurations")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-sweeps", type=int, default=2000)
     ap.add_argument("--batched-shape", default="",
@@ -519,6 +865,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if args.mode == "slab":
+        return slab_arm(args)
     return gpu_arm(args)
 
 

@@ -11,7 +11,7 @@ from conftest import ROOT
 
 def test_reference_arm_prints_one_contract_line():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "3"],
+                          "--steps", "1", "--warmup", "3", "--edge", "48"],
                          capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [x for x in out.stdout.splitlines() if x.startswith("{")]
@@ -29,21 +29,29 @@ def test_reference_arm_prints_one_contract_line():
 
 
 def test_clock_record_summary(tmp_path):
+    """The nvidia-smi fallback's CSV and the summary every GPU line carries:
+    median SM clock, the reasons seen in any sample, the sample count."""
     import bench
 
-    cs = bench.ClockSampler(0)
-    cs.path = str(tmp_path / "clocks.csv")
-    cs.proc = object()  # as if nvidia-smi had run
+    path = tmp_path / "clocks.csv"
     rows = [  # index, sm, max sm, power, active, hw, hw thermal, sw thermal, sw power cap
         "0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
         "0, 1890, 1965, 998.0, 0x4, Not Active, Not Active, Not Active, Active",
         "0, 1845, 1965, 1001.2, 0x4, Not Active, Not Active, Not Active, Active",
         "garbage line",
     ]
-    with open(cs.path, "w") as f:
-        f.write("\n".join(rows) + "\n")
+    path.write_text("\n".join(rows) + "\n")
+    samples, smax = bench.ClockSampler.parse_smi_csv(str(path))
+    assert smax == 1965.0 and len(samples) == 3
+    cs = bench.ClockSampler(0)
+    cs.samples, cs.sm_max, cs.source = samples, smax, "nvidia-smi"
     s = cs.summary()
     assert s == {"sm_mhz": 1890.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"],
-                 "samples": 3}
-    assert cs.summary() == s  # read once, kept
-    assert not os.path.exists(cs.path)
+                 "samples": 3, "source": "nvidia-smi"}
+    assert cs.summary() == s  # computed once, kept
+    # NVML reason bits: hardware slowdown and thermal reasons are named
+    cs = bench.ClockSampler(0)
+    cs.samples = [(1500.0, 0x8 | 0x4), (1600.0, 0x40), (1700.0, 0x0)]
+    cs.sm_max, cs.source = 1965.0, "nvml"
+    assert cs.summary()["reasons"] == ["hw_slowdown", "hw_thermal_slowdown", "sw_power_cap"]
+    assert cs.summary()["sm_mhz"] == 1600.0
