@@ -51,6 +51,7 @@ namespace {
 struct ReplicaDesc {
   LatticeView L;
   SweepGeom G;
+  WalkGeom W;  // column-walk tasks of the replica (W.seg = 0: grid-stride over units)
   MomentGeom M;
   Coupling cp;
   CouplingD cd;
@@ -177,6 +178,13 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   const PhiloxKeys key = philox_keys(D.key0, D.key1);
   const uint32_t replica = D.replica;
   const uint32_t stride = (uint32_t)nct * THREADS;
+  if (FULL && D.W.seg > 0) {
+    const WalkGeom W = D.W;
+    for (uint32_t t = (uint32_t)rank * THREADS + threadIdx.x; t < W.ntasks; t += stride)
+      walk_task<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, step, d, cp, key,
+                                                                     replica, nacc, nflip);
+    return;
+  }
   const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
   const uint32_t per_colour = plane * (uint32_t)L.nk;
   for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units; g += stride) {
@@ -454,11 +462,67 @@ int occupancy_of(int threads) {
   return n;
 }
 
+// Cost of one pass of replica D on `threads` threads and its loop form
+// (sweep_unit.cuh walk_pass_cost).  CHLL_WALK_SEG fixes the segment (0: the
+// unit loop) for measurements.
+double pass_cost(const chll::ReplicaDesc& D, uint32_t threads, uint32_t* seg) {
+  static const int env = [] {
+    const char* e = std::getenv("CHLL_WALK_SEG");
+    return e ? std::atoi(e) : -1;
+  }();
+  const uint32_t ncols = D.G.Q * (uint32_t)D.L.nj;
+  return chll::walk_pass_cost(D.G.units, ncols, (uint32_t)D.L.nk, D.L.ni % 4 == 0, threads, env,
+                              seg);
+}
+
+// CTAs per replica of one wave that make the slowest replica's pass cost as
+// small as possible within `budget` CTAs (every replica gets at least one):
+// a bisection on the cost bound, each replica taking the fewest CTAs whose
+// cost meets it.  CTAs left over stay idle.
+std::vector<int> split_ctas(const chll_batch* B, const std::vector<int>& reps, int budget) {
+  const int n = (int)reps.size();
+  const int threads = B->threads;
+  std::vector<std::vector<double>> cost(n);  // cost[t][c-1]: replica t on c CTAs
+  std::vector<double> cand;
+  for (int t = 0; t < n; ++t) {
+    const chll::ReplicaDesc& D = B->desc[reps[t]];
+    const int cap = std::max(1, std::min(budget - (n - 1),
+                                         (int)((D.G.units + threads - 1) / threads)));
+    for (int c = 1; c <= cap; ++c) {
+      uint32_t seg;
+      cost[t].push_back(pass_cost(D, (uint32_t)(c * threads), &seg));
+      cand.push_back(cost[t].back());
+    }
+  }
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  auto need = [&](double bound, std::vector<int>* out) {
+    long long total = 0;
+    for (int t = 0; t < n; ++t) {
+      int c = 1;
+      while (c < (int)cost[t].size() && cost[t][c - 1] > bound) ++c;
+      if (cost[t][c - 1] > bound) return (long long)budget + 1;  // bound not reachable
+      if (out) (*out)[t] = c;
+      total += c;
+    }
+    return total;
+  };
+  size_t lo = 0, hi = cand.size() - 1;  // the largest candidate always fits
+  while (lo < hi) {
+    const size_t mid = (lo + hi) / 2;
+    if (need(cand[mid], nullptr) <= budget) hi = mid;
+    else lo = mid + 1;
+  }
+  std::vector<int> cnt(n, 1);
+  need(cand[lo], &cnt);
+  return cnt;
+}
+
 // Splits the replicas into waves whose float4 state together stays within
-// wave_bytes (0: one wave), largest replicas first, and gives every replica of
-// a wave CTAs in proportion to its units (at least one, at most one per
-// `threads` units) out of the whole co-resident grid.  Fills
-// desc[].cta_first/cta_count and the per-wave CTA map (-1: idle).
+// wave_bytes (0: one wave), largest replicas first, and gives the replicas of
+// a wave CTAs out of the whole co-resident grid (split_ctas) with each
+// replica's loop form (pass_cost).  Fills desc[].cta_first/cta_count/W and
+// the per-wave CTA map (-1: idle).
 int shape_launch(chll_batch* B) {
   if (B->shape_threads == B->threads && B->shape_ctas == B->ctas_per_sm &&
       B->shape_wave_bytes == B->wave_bytes && B->grid > 0)
@@ -501,31 +565,14 @@ int shape_launch(chll_batch* B) {
   for (size_t w = 0; w < waves.size(); ++w) {
     const std::vector<int>& reps = waves[w];
     const int n = (int)reps.size();
-    double tot = 0.0;
-    for (int r : reps) tot += (double)B->desc[r].G.units;
-    std::vector<int> cnt(n, 1), cap(n);
-    for (int t = 0; t < n; ++t)
-      cap[t] = std::max(1, (int)((B->desc[reps[t]].G.units + B->threads - 1) / B->threads));
-    int used = n;
-    const int extra = budget - n;
-    std::vector<std::pair<double, int>> rem;
-    for (int t = 0; t < n; ++t) {
-      const double want = extra * (double)B->desc[reps[t]].G.units / tot;
-      const int add = std::min((int)want, cap[t] - 1);
-      cnt[t] += add;
-      used += add;
-      rem.push_back({want - (int)want, t});
-    }
-    std::sort(rem.begin(), rem.end(), [](auto& a, auto& b) { return a.first > b.first; });
-    for (auto& pr : rem) {
-      if (used >= budget) break;
-      if (cnt[pr.second] < cap[pr.second]) {
-        ++cnt[pr.second];
-        ++used;
-      }
-    }
+    const std::vector<int> cnt = split_ctas(B, reps, budget);
     int next = 0;
     for (int t = 0; t < n; ++t) {
+      chll::ReplicaDesc& D = B->desc[reps[t]];
+      uint32_t seg = 0;
+      pass_cost(D, (uint32_t)(cnt[t] * B->threads), &seg);
+      D.W = chll::make_walk(D.G, D.L, seg ? seg : 1);
+      if (!seg) D.W.seg = 0;
       B->desc[reps[t]].cta_first = next;
       B->desc[reps[t]].cta_count = cnt[t];
       for (int c = 0; c < cnt[t]; ++c) map[w * (size_t)budget + next++] = reps[t];
@@ -903,10 +950,12 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
   int bt = keep_threads, bc = keep_ctas;
   int rc = CHLL_OK;
   long long bw = B->wave_bytes;
-  // Candidates: one wave or 48 MiB waves; each block size at its two highest
+  // Candidates: one wave, or waves of 40, 64 or 96 MiB of state (a wave that
+  // fits in the 126 MB L2 runs its sweeps from L2, at the price of fewer
+  // replicas sharing the grid); each block size at its two highest
   // occupancies (lower occupancies were never faster on this kernel).  Trials
   // measure every 10 sweeps like a production run.
-  const long long kWaveOptions[] = {0ll, 48ll << 20};
+  const long long kWaveOptions[] = {0ll, 40ll << 20, 64ll << 20, 96ll << 20};
   for (long long wb : kWaveOptions)
   for (int threads : {128, 256, 512}) {
     const int occ = occupancy_of(threads);

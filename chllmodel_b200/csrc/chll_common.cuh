@@ -99,10 +99,28 @@ __host__ __device__ __forceinline__ float u01(uint32_t x) {
   return (float)(x >> 8) * 5.9604644775390625e-8f;  // 2^-24
 }
 
+// A float from its bits.
+__host__ __device__ __forceinline__ float float_of_bits(uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  float f;
+  __builtin_memcpy(&f, &b, sizeof f);
+  return f;
+#endif
+}
+
+// b * 2^-16 - 1/2 for a 16-bit b given as b << 7: the float 1 + b * 2^-16 is
+// assembled from its bits (the exponent of 1, b at the top of the mantissa)
+// and 1.5 subtracted, both exact, with no integer-to-float conversion.
+__host__ __device__ __forceinline__ float centred_u16(uint32_t b16_shl7) {
+  return float_of_bits(0x3f800000u | b16_shl7) - 1.5f;
+}
+
 // The uniforms of one block and colour from its sweep call (see above).
 struct UnitRandoms {
   float acc[2];   // director acceptance
-  float ang[2];   // director angle (16-bit)
+  float ang[2];   // director angle uniform u minus 1/2 (16-bit u), in [-1/2, 1/2)
   float flip[2];  // chirality-flip acceptance
 };
 
@@ -110,8 +128,8 @@ __host__ __device__ __forceinline__ UnitRandoms unit_randoms(const Ctr4& r) {
   UnitRandoms u;
   u.acc[0] = u01(r.v[0]);
   u.acc[1] = u01(r.v[1]);
-  u.ang[0] = (float)(r.v[2] >> 16) * 1.52587890625e-5f;      // 2^-16
-  u.ang[1] = (float)(r.v[2] & 0xffffu) * 1.52587890625e-5f;
+  u.ang[0] = centred_u16((r.v[2] >> 9) & 0x007fff80u);  // high 16 bits of v2
+  u.ang[1] = centred_u16((r.v[2] << 7) & 0x007fff80u);  // low 16 bits
   u.flip[0] = u01(r.v[3]);
   u.flip[1] = (float)(((r.v[3] & 0xffu) << 16) | ((r.v[0] & 0xffu) << 8) | (r.v[1] & 0xffu)) *
               5.9604644775390625e-8f;

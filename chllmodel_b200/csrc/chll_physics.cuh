@@ -30,11 +30,12 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 // the reference) is exactly |nz| >= 0.999f for an FP32 nz.
 // The angle is taken as psi = 2*pi*(u - 1/2) in [-pi, pi), where the hardware
 // sine/cosine have absolute error <= 2^-21.4, and sin(phi) = -sin(psi),
-// cos(phi) = -cos(psi); u - 1/2 is exact for the 16-bit angle uniform.
-__device__ __forceinline__ void propose_director(float nx, float ny, float nz, float d, float u,
+// cos(phi) = -cos(psi).  uc = u - 1/2 (UnitRandoms.ang) is exact for the
+// 16-bit angle uniform.
+__device__ __forceinline__ void propose_director(float nx, float ny, float nz, float d, float uc,
                                                  float& mx, float& my, float& mz) {
   float sn, cs;
-  __sincosf(__fmul_rn(6.28318530717958647692f, u - 0.5f), &sn, &cs);
+  __sincosf(__fmul_rn(6.28318530717958647692f, uc), &sn, &cs);
   const float a = -__fmul_rn(d, cs), bb = -__fmul_rn(d, sn);  // d cos(phi), d sin(phi)
   float x, y, z;
   if (fabsf(nz) >= 0.999f) {

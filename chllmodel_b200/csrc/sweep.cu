@@ -18,6 +18,7 @@
 // chll_mod.f90:83-93 on the device: paccept and the d adaptation after the
 // second director pass, faccept and the step increment after the second flip
 // pass.
+#include <cstdlib>
 #include <mutex>
 
 #include "chll_common.cuh"
@@ -175,9 +176,12 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 // peer: the halo planes of neighbouring z-slabs that this slab's boundary
 // planes are written to (null pointers for a whole lattice).  The periodic
 // whole-lattice mode has no peers.
-template <int PHASE, int BMODE, bool FULL>
+// FORM: 0 = grid-stride over units with padding checks, 1 = grid-stride, ni a
+// multiple of 4 (no padding), 2 = column walk (sweep_unit.cuh walk_task), ni a
+// multiple of 4.
+template <int PHASE, int BMODE, int FORM>
 __global__ void __launch_bounds__(kThreads, 2)
-    fused_pass_kernel(LatticeView L, SweepGeom G, Coupling cp, PhiloxKeys keys,
+    fused_pass_kernel(LatticeView L, SweepGeom G, WalkGeom W, Coupling cp, PhiloxKeys keys,
                       uint32_t replica, Control* __restrict__ ctl, PeerPlanes peer) {
   constexpr int C = PHASE == kFusedB ? 1 : 0;
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
@@ -185,13 +189,26 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr bool FLIP_AFTER = PHASE == kFusedB;
   constexpr bool PXY = BMODE != kBoundOpen;
   constexpr bool PZ = BMODE == kBoundPeriodic;
+  constexpr bool FULL = FORM != 0;
   const long long step = ctl->step;
   const float d = (float)ctl->d;
   unsigned int nacc = 0, nflip = 0;
   const uint32_t stride = gridDim.x * kThreads;
   const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
   const uint32_t per_colour = plane * (uint32_t)L.nk;
-  if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
+  if (FORM == 2) {
+    if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
+      for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < W.ntasks; t += stride)
+        walk_task<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
+                                                            replica, nacc, nflip);
+    } else {
+      for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < W.ntasks; t += stride)
+        walk_task<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
+                                                            replica, nacc, nflip, peer);
+      // the halo stores reach the other GPU before this kernel counts as done
+      __threadfence_system();
+    }
+  } else if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
     for (uint32_t g = G.first + blockIdx.x * kThreads + threadIdx.x; g < G.units; g += stride) {
       if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
       unit_step<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER, FULL>(L, G, g, (uint32_t)step, d, cp,
@@ -259,18 +276,19 @@ const StagedKernel kStaged[2][4] = {
     {staged_pass_kernel<true, 0, true>, staged_pass_kernel<true, 1, true>,
      staged_pass_kernel<false, 0, true>, staged_pass_kernel<false, 1, true>}};
 
-using FusedKernel = void (*)(LatticeView, SweepGeom, Coupling, PhiloxKeys, uint32_t, Control*,
-                            PeerPlanes);
+using FusedKernel = void (*)(LatticeView, SweepGeom, WalkGeom, Coupling, PhiloxKeys, uint32_t,
+                            Control*, PeerPlanes);
 
-// [boundary mode][phase][ni a multiple of 4]
-#define CHLL_FUSED_ROW(M)                                                                       \
-  {{fused_pass_kernel<kFusedA0, M, false>, fused_pass_kernel<kFusedA0, M, true>},               \
-   {fused_pass_kernel<kFusedA, M, false>, fused_pass_kernel<kFusedA, M, true>},                 \
-   {fused_pass_kernel<kFusedB, M, false>, fused_pass_kernel<kFusedB, M, true>},                 \
-   {fused_pass_kernel<kFusedF, M, false>, fused_pass_kernel<kFusedF, M, true>}}
-const FusedKernel kFused[3][4][2] = {CHLL_FUSED_ROW(kBoundOpen), CHLL_FUSED_ROW(kBoundPeriodic),
+// [boundary mode][phase][form]
+#define CHLL_FUSED_PHASE(P, M) \
+  {fused_pass_kernel<P, M, 0>, fused_pass_kernel<P, M, 1>, fused_pass_kernel<P, M, 2>}
+#define CHLL_FUSED_ROW(M)                                                            \
+  {CHLL_FUSED_PHASE(kFusedA0, M), CHLL_FUSED_PHASE(kFusedA, M), CHLL_FUSED_PHASE(kFusedB, M), \
+   CHLL_FUSED_PHASE(kFusedF, M)}
+const FusedKernel kFused[3][4][3] = {CHLL_FUSED_ROW(kBoundOpen), CHLL_FUSED_ROW(kBoundPeriodic),
                                      CHLL_FUSED_ROW(kBoundSlabXY)};
 #undef CHLL_FUSED_ROW
+#undef CHLL_FUSED_PHASE
 
 // Largest dynamic shared memory a staged CTA may ask for (2 stages).
 constexpr size_t kStagedSmemMax = 200 * 1024;
@@ -281,7 +299,7 @@ constexpr size_t kStagedSmemMax = 200 * 1024;
 struct DeviceShape {
   int sms = 0;
   int per_sm[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  int fused_per_sm[3][4][2] = {};
+  int fused_per_sm[3][4][3] = {};
   size_t staged_smem[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last size asked per kernel
   int staged_per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
@@ -307,7 +325,7 @@ DeviceShape& device_shape() {
     for (int per = 0; per < 2; ++per)
       for (int p = 0; p < 4; ++p) {
         s.per_sm[per][p] = occupancy(kKernels[per][p]);
-        for (int f = 0; f < 2; ++f) {
+        for (int f = 0; f < 3; ++f) {
           s.fused_per_sm[per][p][f] = occupancy(kFused[per][p][f]);
           if (per == 1) s.fused_per_sm[2][p][f] = occupancy(kFused[2][p][f]);
         }
@@ -328,6 +346,21 @@ int staged_occupancy(DeviceShape& ds, int per, int pass, size_t smem) {
     ds.staged_per_sm[idx] = n > 0 ? n : 1;
   }
   return ds.staged_per_sm[idx];
+}
+
+// Planes per column-walk task for a launch of `threads` resident threads, or
+// 0 for the grid-stride unit loop (walk_pass_cost).  CHLL_WALK_SEG fixes the
+// segment (0: the unit loop) for measurements.
+uint32_t walk_segment(const SweepGeom& G, const LatticeView& L, uint32_t threads) {
+  static const int env = [] {
+    const char* e = std::getenv("CHLL_WALK_SEG");
+    return e ? std::atoi(e) : -1;
+  }();
+  const uint32_t ncols = G.Q * (uint32_t)L.nj;
+  uint32_t seg = 0;
+  walk_pass_cost(G.units - G.first, ncols, ncols ? (G.units - G.first) / ncols : 0,
+                 L.ni % 4 == 0, threads, env, &seg);
+  return seg;
 }
 
 }  // namespace
@@ -377,10 +410,14 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
                        cudaStream_t stream, float4* peer_lo, float4* peer_hi) {
   DeviceShape& ds = device_shape();
   const int m = bmode < 0 ? 0 : (bmode > 2 ? 2 : bmode);
-  const uint32_t n = G.units - G.first;
-  const uint32_t need = (n + kThreads - 1) / kThreads;
   const int full = L.ni % 4 == 0;
-  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3][full];
+  const uint32_t res_walk = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3][2];
+  const uint32_t seg = full ? walk_segment(G, L, res_walk * kThreads) : 0;
+  const int form = seg ? 2 : full;
+  const WalkGeom W = make_walk(G, L, seg ? seg : 1);
+  const uint32_t n = form == 2 ? W.ntasks : G.units - G.first;
+  const uint32_t need = (n + kThreads - 1) / kThreads;
+  const uint32_t resident = (uint32_t)ds.sms * (uint32_t)ds.fused_per_sm[m][phase & 3][form];
   const dim3 grid(need < resident ? (need ? need : 1) : resident);
   // The first and last planes of the unit range: slots 2*first .. and the
   // plane before slot 2*units.
@@ -390,7 +427,7 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
   peer.hi = m == kBoundPeriodic ? nullptr : peer_hi;
   peer.lo_first = 2 * G.first;
   peer.hi_first = 2 * G.units - peer.plane;
-  kFused[m][phase & 3][full]<<<grid, kThreads, 0, stream>>>(L, G, cp, philox_keys(key0, key1),
+  kFused[m][phase & 3][form]<<<grid, kThreads, 0, stream>>>(L, G, W, cp, philox_keys(key0, key1),
                                                              replica, ctl, peer);
 }
 

@@ -232,6 +232,184 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
   peer.store(2 * g, U.n0, U.n1);
 }
 
+// ---------------------------------------------------------------------------
+// Column walk (lattices whose ni is a multiple of 4, so no unit holds a
+// padding slot).  A task is one column of units -- unit q of row j -- over a
+// run of consecutive planes [k0, k1); a thread walks it plane by plane.  The
+// other colour's unit pair q of row (j, k) serves three consecutive steps:
+// as the +z pair of plane k-1, the x-row pair of plane k and the -z pair of
+// plane k+1, so it is loaded once and carried in registers.  Per step the
+// thread loads its own pair, the +y, -y and +z pairs and one x neighbour
+// that lies outside pair q, with offsets fixed for the whole column: no
+// per-unit index decode and no boundary tests other than the z ends.  Units,
+// counters and arithmetic are those of unit_step, so the chain is the same
+// bit for bit.
+//
+// Which x neighbours pair q supplies: in row (j, k) the pass's colour has
+// parity o = (C+j+k)&1 and its unit q holds sites i0 = 4q+o, i1 = i0+2; the
+// other colour's pair q holds 4q+1-o, 4q+3-o.  For o = 0 that is i0+1 and
+// i1+1 (+x of i0 and i1, and -x of i1), the extra one being i0-1 (slot 2q-1,
+// or the row's last slot across a periodic x edge); for o = 1 it is i0-1
+// and i0+1 (-x of i0 and i1, and +x of i0), the extra one being i1+1 (slot
+// 2q+2, or slot 0 across the edge).  The y and z neighbour pairs are pair q
+// of rows (j+-1, k) and (j, k+-1), which have parity o as well.
+// ---------------------------------------------------------------------------
+struct WalkGeom {
+  uint32_t Q;        // units per row
+  uint32_t ncols;    // columns (units per plane): Q * nj
+  uint32_t seg;      // planes per task (the last task of a column may have fewer)
+  uint32_t nseg;     // tasks per column
+  uint32_t ntasks;   // ncols * nseg
+  uint32_t k_first;  // planes walked: [k_first, k_end)
+  uint32_t k_end;
+  uint32_t goff;     // added to a unit's index for its random counter (mod 2^32)
+  FastDiv by_cols;   // task -> segment
+  FastDiv by_Q;      // column -> row
+};
+
+// The walk of the unit range of G (whole planes) in tasks of `seg` planes.
+__host__ inline WalkGeom make_walk(const SweepGeom& G, const LatticeView& L, uint32_t seg) {
+  WalkGeom W;
+  W.Q = G.Q;
+  W.ncols = G.Q * (uint32_t)L.nj;
+  W.k_first = G.first / W.ncols;
+  W.k_end = G.units / W.ncols;
+  const uint32_t planes = W.k_end - W.k_first;
+  W.seg = seg < 1 ? 1 : (seg > planes ? planes : seg);
+  W.nseg = planes ? (planes + W.seg - 1) / W.seg : 0;
+  W.ntasks = W.ncols * W.nseg;
+  W.goff = G.goff;
+  W.by_cols = FastDiv(W.ncols);
+  W.by_Q = FastDiv(W.Q);
+  return W;
+}
+
+// Cost of one pass of `units` units (ncols columns of `planes` planes) on
+// `threads` threads: about the most work any thread does, counted in
+// grid-stride units.  A walk step costs kWalkStep of a grid-stride unit (no
+// index decode, two loads fewer) and a task kWalkPrime more (its first x-row
+// and -z loads); whole tasks per thread quantise more coarsely than units.
+// *seg: planes per task of the cheapest walk, or 0 when the grid-stride unit
+// loop is cheaper or ni is not a multiple of 4 (full = false).
+// force_seg >= 0 fixes the segment instead (0: the unit loop).
+constexpr double kWalkStep = 0.9, kWalkPrime = 0.3;
+
+__host__ inline double walk_pass_cost(uint32_t units, uint32_t ncols, uint32_t planes, bool full,
+                                      uint32_t threads, int force_seg, uint32_t* seg) {
+  double best = (double)((units + threads - 1) / (threads ? threads : 1));
+  *seg = 0;
+  if (!full || force_seg == 0 || ncols == 0) return best;
+  for (uint32_t s = 2; s <= planes; ++s) {
+    if (force_seg > 0 && s != (uint32_t)force_seg) continue;
+    const uint64_t tasks = (uint64_t)ncols * ((planes + s - 1) / s);
+    const double cost =
+        (double)((tasks + threads - 1) / threads) * ((double)s * kWalkStep + kWalkPrime);
+    if (cost < best || force_seg > 0) {
+      best = cost;
+      *seg = s;
+    }
+  }
+  return best;
+}
+
+// One task of the column walk: trials FLIP_BEFORE / DIR / FLIP_AFTER of
+// unit_trials on every unit of column t % ncols over its planes.
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY,
+          class PEER = NoPeer>
+__device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& W, uint32_t t,
+                                          uint32_t step, float d, const Coupling& cp,
+                                          const KEY& key, uint32_t replica, unsigned int& nacc,
+                                          unsigned int& nflip, const PEER& peer = PEER()) {
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t sg = W.by_cols.div(t);
+  const uint32_t col = t - sg * W.ncols;
+  const uint32_t j = W.by_Q.div(col);
+  const uint32_t q = col - j * W.Q;
+  const uint32_t k0 = W.k_first + sg * W.seg;
+  const uint32_t k1 = min(k0 + W.seg, W.k_end);
+  const uint32_t hx = (uint32_t)L.hx, nj = (uint32_t)L.nj, nk = (uint32_t)L.nk;
+  const uint32_t plane = hx * nj;
+  const float4* __restrict__ oth = L.col[C ^ 1];
+  float4* __restrict__ own = L.col[C];
+
+  // Slot offsets from the unit's own slot, fixed per column (two's
+  // complement for negative offsets).
+  const bool hyp = PXY || j + 1 < nj, hym = PXY || j > 0;
+  const uint32_t oyp = j + 1 < nj ? hx : (uint32_t)(-(int32_t)((nj - 1) * hx));
+  const uint32_t oym = j > 0 ? (uint32_t)(-(int32_t)hx) : (nj - 1) * hx;
+  // the extra x neighbour: parity 0 -> slot 2q-1 (q = 0: the row's last
+  // slot), parity 1 -> slot 2q+2 (q = Q-1: slot 0)
+  const bool hx0 = PXY || q > 0, hx1 = PXY || q + 1 < W.Q;
+  const uint32_t ox0 = q > 0 ? (uint32_t)-1 : 2 * W.Q - 1;
+  const uint32_t ox1 = q + 1 < W.Q ? 2u : (uint32_t)(-(int32_t)(2 * q));
+
+  uint32_t u = (k0 * nj + j) * hx + 2 * q;  // own slot of the current step
+  uint32_t g = col + W.ncols * k0;          // unit index
+  uint32_t o = (C + j + k0) & 1u;
+
+  // pair q of the x-row (j, k0) and of the row below (j, k0 - 1)
+  float4 xa, xb, za, zb;
+  {
+    const UnitSlots x = ld_unit_nc(oth + u);
+    xa = x.a;
+    xb = x.b;
+  }
+  if (PZ || k0 > 0) {
+    const UnitSlots z = ld_unit_nc(oth + (k0 > 0 ? u - plane : u + (nk - 1) * plane));
+    za = z.a;
+    zb = z.b;
+  } else {
+    za = zb = zero;
+  }
+  for (uint32_t k = k0; k < k1; ++k) {
+    const bool hzp = PZ || k + 1 < nk;
+    const uint32_t ozp = k + 1 < nk ? plane : (uint32_t)(-(int32_t)((nk - 1) * plane));
+    if (k + 1 < k1) {
+      // the next step's own pair and +z pair, the lines no thread has read yet
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(own + u + plane));
+      if (k + 2 < nk) asm volatile("prefetch.global.L1 [%0];" ::"l"(oth + u + 2 * plane));
+    }
+    UnitNbhd U;
+    U.cen = own + u;
+    const UnitSlots ow = ld_unit(U.cen);
+    U.n0 = ow.a;
+    U.n1 = ow.b;
+    nbr_units(hyp, oth + u + oyp, U.nb0.b[2], U.nb1.b[2]);
+    nbr_units(hym, oth + u + oym, U.nb0.b[3], U.nb1.b[3]);
+    float4 pa, pb;  // +z pair: the next step's x-row pair
+    nbr_units(hzp, oth + u + ozp, pa, pb);
+    U.nb0.b[4] = pa;
+    U.nb1.b[4] = pb;
+    U.nb0.b[5] = za;
+    U.nb1.b[5] = zb;
+    if (o == 0) {
+      const float4 e = hx0 ? ld4(oth + u + ox0) : zero;
+      U.nb0.b[0] = xa;  // +x of i0
+      U.nb0.b[1] = e;   // -x of i0
+      U.nb1.b[0] = xb;  // +x of i1
+      U.nb1.b[1] = xa;  // -x of i1
+    } else {
+      const float4 e = hx1 ? ld4(oth + u + ox1) : zero;
+      U.nb0.b[0] = xb;  // +x of i0
+      U.nb0.b[1] = xa;  // -x of i0
+      U.nb1.b[0] = e;   // +x of i1
+      U.nb1.b[1] = xb;  // -x of i1
+    }
+    unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(U.n0, U.n1, U.nb0, U.nb1, true, true,
+                                                 g + W.goff, step, d, cp, key, replica, nacc,
+                                                 nflip);
+    st_unit(U.cen, U.n0, U.n1);
+    peer.store(u, U.n0, U.n1);
+    za = xa;
+    zb = xb;
+    xa = pa;
+    xb = pb;
+    u += plane;
+    g += W.ncols;
+    o ^= 1u;
+  }
+}
+
 // One of the reference's four half-sweeps on unit g; returns the number of
 // accepted trials (0..2).
 template <bool DIRECTOR, int C, bool PERIODIC>

@@ -95,6 +95,37 @@ def test_lockstep_half_sweeps(oracle, shape, periodic, kT, K, g, eps):
     assert ties <= max(2, decided // 2000)
 
 
+@pytest.mark.parametrize("periodic", [False, True])
+def test_lockstep_reference_size_run(oracle, periodic):
+    """The 32^3 reference-size configuration itself (K = 0.5, h = 0,
+    kT = 0.5, d0 = 0.1, seed 1 for the initial state and the sweeps), open
+    as the reference's sweep and periodic, four sweeps in lockstep; then the
+    library's fused sweep from the same start reaches the four half-sweeps'
+    final GPU state and control block bit for bit."""
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    shape, nsw = (32, 32, 32), 4
+    ties, decided = lockstep(oracle, shape, periodic, 0.5, 0.5, 0.0, sweeps=nsw, seed=1,
+                             d0=0.1, init_seed=1)
+    assert decided == 32 ** 3 * 2 * nsw
+    assert ties <= max(2, decided // 2000)
+    bnd = "periodic" if periodic else "open"
+    nx, ny, nz, s = oracle.init_random(oracle.make_cfg(*shape, seed=1))
+    four, fused = Lattice(*shape, boundary=bnd), Lattice(*shape, boundary=bnd)
+    cp = coupling(0.5, 0.5, 0.0)
+    for lat in (four, fused):
+        lat.upload_f64(nx, ny, nz, s)
+        lat.set_control(0.1, step=1)
+    for _ in range(nsw):
+        for p in range(4):
+            four.half_sweep(cp, p, seed=1)
+    fused.sweep(cp, nsw, seed=1)
+    assert np.array_equal(four.download_f4(), fused.download_f4())
+    assert four.control() == fused.control()
+    four.close()
+    fused.close()
+
+
 def test_zero_temperature_rule(oracle):
     ties, decided = lockstep(oracle, (8, 8, 6), False, 0.0, 1.0, 0.5, sweeps=2)
     assert ties <= 2
