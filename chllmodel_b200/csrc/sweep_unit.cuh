@@ -332,8 +332,9 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
   const float4* __restrict__ oth = L.col[C ^ 1];
   float4* __restrict__ own = L.col[C];
 
-  // Slot offsets from the unit's own slot, fixed per column (two's
-  // complement for negative offsets).
+  // Slot offsets from the unit's own slot, fixed per column: two's
+  // complement for negative offsets, so every address is formed as
+  // base + (u + offset) with the sum wrapping in 32 bits to the slot index.
   const bool hyp = PXY || j + 1 < nj, hym = PXY || j > 0;
   const uint32_t oyp = j + 1 < nj ? hx : (uint32_t)(-(int32_t)((nj - 1) * hx));
   const uint32_t oym = j > 0 ? (uint32_t)(-(int32_t)hx) : (nj - 1) * hx;
@@ -366,30 +367,30 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
     const uint32_t ozp = k + 1 < nk ? plane : (uint32_t)(-(int32_t)((nk - 1) * plane));
     if (k + 1 < k1) {
       // the next step's own pair and +z pair, the lines no thread has read yet
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(own + u + plane));
-      if (k + 2 < nk) asm volatile("prefetch.global.L1 [%0];" ::"l"(oth + u + 2 * plane));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(own + (u + plane)));
+      if (k + 2 < nk) asm volatile("prefetch.global.L1 [%0];" ::"l"(oth + (u + 2 * plane)));
     }
     UnitNbhd U;
     U.cen = own + u;
     const UnitSlots ow = ld_unit(U.cen);
     U.n0 = ow.a;
     U.n1 = ow.b;
-    nbr_units(hyp, oth + u + oyp, U.nb0.b[2], U.nb1.b[2]);
-    nbr_units(hym, oth + u + oym, U.nb0.b[3], U.nb1.b[3]);
+    nbr_units(hyp, oth + (u + oyp), U.nb0.b[2], U.nb1.b[2]);
+    nbr_units(hym, oth + (u + oym), U.nb0.b[3], U.nb1.b[3]);
     float4 pa, pb;  // +z pair: the next step's x-row pair
-    nbr_units(hzp, oth + u + ozp, pa, pb);
+    nbr_units(hzp, oth + (u + ozp), pa, pb);
     U.nb0.b[4] = pa;
     U.nb1.b[4] = pb;
     U.nb0.b[5] = za;
     U.nb1.b[5] = zb;
     if (o == 0) {
-      const float4 e = hx0 ? ld4(oth + u + ox0) : zero;
+      const float4 e = hx0 ? ld4(oth + (u + ox0)) : zero;
       U.nb0.b[0] = xa;  // +x of i0
       U.nb0.b[1] = e;   // -x of i0
       U.nb1.b[0] = xb;  // +x of i1
       U.nb1.b[1] = xa;  // -x of i1
     } else {
-      const float4 e = hx1 ? ld4(oth + u + ox1) : zero;
+      const float4 e = hx1 ? ld4(oth + (u + ox1)) : zero;
       U.nb0.b[0] = xb;  // +x of i0
       U.nb0.b[1] = xa;  // -x of i0
       U.nb1.b[0] = e;   // +x of i1
