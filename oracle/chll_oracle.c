@@ -346,6 +346,37 @@ int oracle_run(const oracle_cfg* c, int nstart, int nstop, int nout, long long a
   return mc;
 }
 
+/* An equilibrium chain of the same step loop, for the statistical parity
+ * tests: sweeps istep = 1 .. burn + nmeas*every with the d rule while
+ * istep < adapt_until, and after sweep burn, every `every` sweeps, the nine
+ * FP64 moments of oracle_moments appended to out (nmeas x 9).  *d is the
+ * proposal amplitude in and out. */
+int oracle_chain(const oracle_cfg* c, int burn, int nmeas, int every, long long adapt_until,
+                 double* d, double* nx, double* ny, double* nz, int* s, double* out) {
+  const long long n3 = (long long)c->ni * c->nj * c->nk;
+  const int total = burn + nmeas * every;
+  int mc = 0;
+  for (int istep = 1; istep <= total; ++istep) {
+    long long naccept = 0;
+    naccept += oracle_pass(c, 0, (uint32_t)istep, *d, nx, ny, nz, s, NULL, NULL, NULL);
+    naccept += oracle_pass(c, 1, (uint32_t)istep, *d, nx, ny, nz, s, NULL, NULL, NULL);
+    oracle_pass(c, 2, (uint32_t)istep, *d, nx, ny, nz, s, NULL, NULL, NULL);
+    oracle_pass(c, 3, (uint32_t)istep, *d, nx, ny, nz, s, NULL, NULL, NULL);
+    const double paccept = (double)((float)naccept / (float)n3);
+    if (istep < adapt_until) {
+      if (paccept < 0.4)
+        *d = *d * (double)0.995f;
+      else if (paccept > 0.6)
+        *d = *d / (double)0.995f;
+    }
+    if (istep > burn && (istep - burn) % every == 0 && mc < nmeas) {
+      oracle_moments(c, nx, ny, nz, s, out + 9 * (size_t)mc);
+      ++mc;
+    }
+  }
+  return mc;
+}
+
 /* Random initial state on the device's stream: counter {site, 0xffffffff,
  * replica, 4}; cos(theta) = 2u0-1, phi = 2*pi*u1, s = -1 if u2 < 1/2. */
 void oracle_init_random(const oracle_cfg* c, double* nx, double* ny, double* nz, int* s) {

@@ -72,6 +72,9 @@ def lib():
                              P(ct.c_double), d_arr, d_arr, d_arr, i_arr, ct.c_void_p,
                              ct.c_void_p, ct.c_int]
     L.oracle_run.restype = ct.c_int
+    L.oracle_chain.argtypes = [P(Cfg), ct.c_int, ct.c_int, ct.c_int, ct.c_longlong,
+                               P(ct.c_double), d_arr, d_arr, d_arr, i_arr, ct.c_void_p]
+    L.oracle_chain.restype = ct.c_int
     L.oracle_init_random.argtypes = [P(Cfg), d_arr, d_arr, d_arr, i_arr]
     L.oracle_init_random.restype = None
     L.oracle_energy_grad.argtypes = [P(Cfg), d_arr, d_arr, d_arr, i_arr, ct.c_void_p,
@@ -155,6 +158,17 @@ def run(cfg, nstart, nstop, nout, d, nx, ny, nz, s, adapt_until=10000):
     nmeas = lib().oracle_run(ct.byref(cfg), nstart, nstop, nout, int(adapt_until), ct.byref(dd),
                              nx, ny, nz, s, _ptr(msteps), _ptr(m), rows)
     return msteps[:rows], m[:rows], dd.value, nmeas
+
+
+def chain(cfg, burn, nmeas, every, d, nx, ny, nz, s, adapt_until=10000):
+    """An equilibrium chain from step 1 (the reference step loop with its d
+    rule): returns (nmeas x 9 FP64 moments after sweep burn, every `every`
+    sweeps, as moments() gives them; the final d)."""
+    out = np.zeros((nmeas, 9), np.float64)
+    dd = ct.c_double(d)
+    got = lib().oracle_chain(ct.byref(cfg), int(burn), int(nmeas), int(every), int(adapt_until),
+                             ct.byref(dd), nx, ny, nz, s, _ptr(out))
+    return out[:got], dd.value
 
 
 def init_random(cfg):
