@@ -504,10 +504,8 @@ def gpu_arm(args):
     return 0
 
 
-def _events(torch, stream):
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    return a, b
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
 def other_configs(args, torch):
@@ -586,7 +584,7 @@ def other_configs(args, torch):
     # (seed 3), the energy adjoint (dE/dn and dE/d(eps, K, h)), a 2000-step
     # zero-temperature gradient quench.
     e = 64
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # not the default stream, whose handle 0 means the lattice's own
     lat = Lattice(e, e, e, boundary="periodic")
     lat.set_stream(stream.cuda_stream)
     lat.init_random(3)
@@ -595,13 +593,14 @@ def other_configs(args, torch):
     lat.sweep(cpe, 10, seed=3)  # graph capture
     lat.init_random(3)
     lat.set_control(0.1, step=1)
-    a, b = _events(torch, stream)
+    a, b = _events(torch)
     a.record(stream)
     lat.sweep(cpe, 500, seed=3)
     b.record(stream)
     b.synchronize()
     t_eq = a.elapsed_time(b) * 1e-3
-    grad = torch.empty((e ** 3, 4), dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        grad = torch.empty((e ** 3, 4), dtype=torch.float32, device="cuda")
     cpq = coupling(0.0, 1.0, 0.5)
     lat.energy_grad(cpq, project=True, grad_ptr=grad.data_ptr())  # allocation
     reps = 20

@@ -287,12 +287,14 @@ __host__ inline WalkGeom make_walk(const SweepGeom& G, const LatticeView& L, uin
 // Cost of one pass of `units` units (ncols columns of `planes` planes) on
 // `threads` threads: about the most work any thread does, counted in
 // grid-stride units.  A walk step costs kWalkStep of a grid-stride unit (no
-// index decode, two loads fewer) and a task kWalkPrime more (its first x-row
-// and -z loads); whole tasks per thread quantise more coarsely than units.
+// index decode, two loads fewer; the 480^3 passes ran at 0.94 of the unit
+// loop's time in 16-plane tasks) and a task kWalkPrime more (its first x-row
+// and -z loads, the column decode); whole tasks per thread quantise more
+// coarsely than units.
 // *seg: planes per task of the cheapest walk, or 0 when the grid-stride unit
 // loop is cheaper or ni is not a multiple of 4 (full = false).
 // force_seg >= 0 fixes the segment instead (0: the unit loop).
-constexpr double kWalkStep = 0.9, kWalkPrime = 0.3;
+constexpr double kWalkStep = 0.93, kWalkPrime = 0.5;
 
 __host__ inline double walk_pass_cost(uint32_t units, uint32_t ncols, uint32_t planes, bool full,
                                       uint32_t threads, int force_seg, uint32_t* seg) {
