@@ -176,6 +176,20 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 // peer: the halo planes of neighbouring z-slabs that this slab's boundary
 // planes are written to (null pointers for a whole lattice).  The periodic
 // whole-lattice mode has no peers.
+// Programmatic dependent launch (sm_90+): the fused passes are launched so
+// that the next pass's grid may be scheduled while this one drains.  Each
+// pass first waits for the grids it depends on to complete and their memory
+// to be visible (griddepcontrol.wait, before any read of the lattice or the
+// control block), and lets its dependents launch once its own units are done
+// (griddepcontrol.launch_dependents, before the count epilogue).  Launches
+// without the attribute ignore both.
+__device__ __forceinline__ void wait_prerequisite_grids() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void allow_dependent_grids() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // FORM: 0 = grid-stride over units with padding checks, 1 = grid-stride, ni a
 // multiple of 4 (no padding), 2 = column walk (sweep_unit.cuh walk_task), ni a
 // multiple of 4.
@@ -190,6 +204,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr bool PXY = BMODE != kBoundOpen;
   constexpr bool PZ = BMODE == kBoundPeriodic;
   constexpr bool FULL = FORM != 0;
+  wait_prerequisite_grids();
   const long long step = ctl->step;
   const float d = (float)ctl->d;
   unsigned int nacc = 0, nflip = 0;
@@ -223,6 +238,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     // the halo stores reach the other GPU before this kernel counts as done
     __threadfence_system();
   }
+  allow_dependent_grids();
   fused_epilogue<PHASE>(ctl, nacc, nflip, step);
 }
 
@@ -427,8 +443,18 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
   peer.hi = m == kBoundPeriodic ? nullptr : peer_hi;
   peer.lo_first = 2 * G.first;
   peer.hi_first = 2 * G.units - peer.plane;
-  kFused[m][phase & 3][form]<<<grid, kThreads, 0, stream>>>(L, G, W, cp, philox_keys(key0, key1),
-                                                             replica, ctl, peer);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kFused[m][phase & 3][form], L, G, W, cp, philox_keys(key0, key1),
+                     replica, ctl, peer);
 }
 
 void launch_fused_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,

@@ -237,13 +237,14 @@ __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom&
 // padding slot).  A task is one column of units -- unit q of row j -- over a
 // run of consecutive planes [k0, k1); a thread walks it plane by plane.  The
 // other colour's unit pair q of row (j, k) serves three consecutive steps:
-// as the +z pair of plane k-1, the x-row pair of plane k and the -z pair of
-// plane k+1, so it is loaded once and carried in registers.  Per step the
-// thread loads its own pair, the +y, -y and +z pairs and one x neighbour
-// that lies outside pair q, with offsets fixed for the whole column: no
-// per-unit index decode and no boundary tests other than the z ends.  Units,
-// counters and arithmetic are those of unit_step, so the chain is the same
-// bit for bit.
+// as the +z pair of plane k-1, the x-row pair of plane k (carried in
+// registers from the step before) and the -z pair of plane k+1 (read again,
+// from L1: carrying it too cost registers that pass B then paid for in
+// recomputed addresses, 5% on its time).  Per step the thread loads its own
+// pair, the +y, -y, +z and -z pairs and one x neighbour that lies outside
+// pair q, with offsets fixed for the whole column: no per-unit index decode
+// and no boundary tests other than the z ends.  Units, counters and
+// arithmetic are those of unit_step, so the chain is the same bit for bit.
 //
 // Which x neighbours pair q supplies: in row (j, k) the pass's colour has
 // parity o = (C+j+k)&1 and its unit q holds sites i0 = 4q+o, i1 = i0+2; the
@@ -350,19 +351,12 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
   uint32_t g = col + W.ncols * k0;          // unit index
   uint32_t o = (C + j + k0) & 1u;
 
-  // pair q of the x-row (j, k0) and of the row below (j, k0 - 1)
-  float4 xa, xb, za, zb;
+  // pair q of the x-row (j, k0)
+  float4 xa, xb;
   {
     const UnitSlots x = ld_unit_nc(oth + u);
     xa = x.a;
     xb = x.b;
-  }
-  if (PZ || k0 > 0) {
-    const UnitSlots z = ld_unit_nc(oth + (k0 > 0 ? u - plane : u + (nk - 1) * plane));
-    za = z.a;
-    zb = z.b;
-  } else {
-    za = zb = zero;
   }
   for (uint32_t k = k0; k < k1; ++k) {
     const bool hzp = PZ || k + 1 < nk;
@@ -383,8 +377,13 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
     nbr_units(hzp, oth + (u + ozp), pa, pb);
     U.nb0.b[4] = pa;
     U.nb1.b[4] = pb;
-    U.nb0.b[5] = za;
-    U.nb1.b[5] = zb;
+    if (PZ || k > 0) {  // -z pair: this thread's x-row pair of the step before, from L1
+      const UnitSlots zr = ld_unit_nc(oth + (k > 0 ? u - plane : u + (nk - 1) * plane));
+      U.nb0.b[5] = zr.a;
+      U.nb1.b[5] = zr.b;
+    } else {
+      U.nb0.b[5] = U.nb1.b[5] = zero;
+    }
     if (o == 0) {
       const float4 e = hx0 ? ld4(oth + (u + ox0)) : zero;
       U.nb0.b[0] = xa;  // +x of i0
@@ -403,8 +402,6 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
                                                  nflip);
     st_unit(U.cen, U.n0, U.n1);
     peer.store(u, U.n0, U.n1);
-    za = xa;
-    zb = xb;
     xa = pa;
     xb = pb;
     u += plane;

@@ -45,9 +45,9 @@ def _check(ni, nj, nk, pxy, pz, C, seg, k_first=0, k_end=None, cols=None):
         u = ((k0 * nj + j) * hx + 2 * q) & M
         g = col + ncols * k0
         o = (C + j + k0) & 1
-        X = u  # x-row pair slot
-        Z = (u - plane) & M if k0 > 0 else ((u + (nk - 1) * plane) & M if pz else None)
+        X = u  # x-row pair slot, carried from step to step
         for k in range(k0, k1):
+            Z = (u - plane) & M if k > 0 else ((u + (nk - 1) * plane) & M if pz else None)
             hzp = pz or k + 1 < nk
             ozp = plane if k + 1 < nk else neg((nk - 1) * plane)
             addrs = {"own": u, "yp": (u + oyp) & M if hyp else None, "ym": (u + oym) & M if hym else None,
@@ -76,7 +76,7 @@ def _check(ni, nj, nk, pxy, pz, C, seg, k_first=0, k_end=None, cols=None):
                     if want != a:
                         raise AssertionError("MISMATCH", (ni, nj, nk, pxy, pz, C, seg), (i, j, k), d, a, want)
                 n += 1
-            Z = X; X = addrs["zp"]
+            X = addrs["zp"]
             u = (u + plane) & M; g += ncols; o ^= 1
     return True
 
