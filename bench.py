@@ -666,9 +666,10 @@ def batched_vs_plain(args, rank, torch):
     b.init_random()
     if args.batched_shape:
         t, c = (int(x) for x in args.batched_shape.split("x"))
-        b.set_tuning(t, c, args.batched_wave_mb << 20)
+        paired = None if args.batched_pairs < 0 else bool(args.batched_pairs)
+        b.set_tuning(t, c, args.batched_wave_mb << 20, paired)
         tune = {"threads": t, "ctas_per_sm": c, "wave_bytes": args.batched_wave_mb << 20,
-                "trial_ms": None}
+                "paired": b.tuning()["paired"], "trial_ms": None}
     else:
         tune = b.autotune(trial_sweeps=200)
     b.run(nsw, measure_every=BATCH_NOUT)   # warm-up: graph capture and first launch
@@ -677,7 +678,7 @@ def batched_vs_plain(args, rank, torch):
     b = Batch(specs)
     b.set_stream(stream.cuda_stream)
     b.init_random()
-    b.set_tuning(tune["threads"], tune["ctas_per_sm"], tune["wave_bytes"])
+    b.set_tuning(tune["threads"], tune["ctas_per_sm"], tune["wave_bytes"], tune["paired"])
     b.sync()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -739,7 +740,7 @@ def batched_vs_plain(args, rank, torch):
             "sequential_chllsim_s": t_sim,
             "speedup_vs_sequential_chllsim": t_sim / t_batched,
             "site_updates_per_s": total * nsw / t_batched,
-            "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "trial_ms")},
+            "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "paired", "trial_ms")},
                            **{"waves": info_tune["waves"],
                               "wave_MiB": info_tune["wave_bytes"] / 2 ** 20}),
             "grid_ctas": info["grid"],
@@ -855,6 +856,9 @@ def main():
                     help="THREADSxCTAS_PER_SM for the batched launch instead of autotuning")
     ap.add_argument("--batched-wave-mb", type=int, default=0,
                     help="wave size with --batched-shape (0: all replicas in one wave)")
+    ap.add_argument("--batched-pairs", type=int, default=-1,
+                    help="with --batched-shape: 1 replica groups of two alternating replicas, "
+                         "0 one replica per group (default: the library's)")
     ap.add_argument("--no-plain-grid", action="store_true",
                     help="skip the sequential plain-kernel grid (profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -137,10 +137,15 @@ class Batch:
                                       ct.byref(g)))
         return {"total_sites": n.value, "replicas": r.value, "threads": t.value, "grid": g.value}
 
-    def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None):
+    def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None, paired=None):
+        """Launch shape (threads per CTA, CTAs per SM; 0: all that fit), wave
+        size in bytes of state (0: one wave) and whether replica groups hold
+        two replicas that alternate their passes (the default) or one."""
         check(self._L.chll_batch_set_tuning(self._h, int(threads), int(ctas_per_sm)))
         if wave_bytes is not None:
             check(self._L.chll_batch_set_wave_bytes(self._h, int(wave_bytes)))
+        if paired is not None:
+            check(self._L.chll_batch_set_pairing(self._h, int(bool(paired))))
 
     def set_wait_limit(self, polls):
         """Polls a replica group's barrier wait makes before it gives up and
@@ -148,11 +153,12 @@ class Batch:
         check(self._L.chll_batch_set_wait_limit(self._h, int(polls)))
 
     def tuning(self) -> dict:
-        t, c, w, n = ct.c_int32(), ct.c_int32(), ct.c_int64(), ct.c_int32()
+        t, c, w, n, p = ct.c_int32(), ct.c_int32(), ct.c_int64(), ct.c_int32(), ct.c_int32()
         check(self._L.chll_batch_get_tuning(self._h, ct.byref(t), ct.byref(c), ct.byref(w),
                                             ct.byref(n)))
+        check(self._L.chll_batch_get_pairing(self._h, ct.byref(p)))
         return {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": w.value,
-                "waves": n.value}
+                "waves": n.value, "paired": bool(p.value)}
 
     def autotune(self, trial_sweeps=20, cache=None) -> dict:
         """Times every launch shape on this replica set and keeps the fastest.
@@ -163,14 +169,16 @@ class Batch:
                 table = json.load(f)
             if key in table:
                 e = table[key]
-                self.set_tuning(e["threads"], e["ctas_per_sm"], e.get("wave_bytes"))
+                self.set_tuning(e["threads"], e["ctas_per_sm"], e.get("wave_bytes"),
+                                e.get("paired"))
                 return dict(e, cached=True)
         t, c, ms = ct.c_int(), ct.c_int(), ct.c_double()
         check(self._L.chll_batch_autotune(self._h, int(trial_sweeps), ct.byref(t), ct.byref(c),
                                           ct.byref(ms)))
         tun = self.tuning()
         res = {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": tun["wave_bytes"],
-               "waves": tun["waves"], "trial_ms": ms.value, "trial_sweeps": int(trial_sweeps)}
+               "waves": tun["waves"], "paired": tun["paired"], "trial_ms": ms.value,
+               "trial_sweeps": int(trial_sweeps)}
         if cache:
             table = {}
             if os.path.exists(cache):

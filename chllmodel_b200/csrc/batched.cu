@@ -97,40 +97,59 @@ __host__ __device__ inline double sym3_max_eig(double a11, double a22, double a3
   return q + 2.0 * p * cos(phi);
 }
 
-// Group barrier of one replica's CTAs.  Returns false if the replica's status
-// word is set (a wait timed out here or in another CTA of the group).
-__device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limit) {
-  __shared__ int s_ok;
+// Group barrier of one replica's CTAs, split in two so that a CTA can do
+// other work between arriving and waiting (a second replica's pass).
+// group_arrive: every thread of the CTA has finished the phase; thread 0
+// publishes the CTA's writes (fence) and counts itself in, the last CTA of
+// the group advancing the generation word.  Returns, in thread 0, the
+// generation to wait past.
+__device__ unsigned int group_arrive(ReplicaState* st, int nct) {
   __syncthreads();
+  unsigned int gen = 0;
+  if (threadIdx.x == 0 && nct > 1) {
+    gen = *(volatile unsigned int*)&st->bar_gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&st->bar_count, 1u);
+    if (arrived == (unsigned int)nct - 1) {
+      st->bar_count = 0;
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    }
+  }
+  return gen;
+}
+
+// Waits until the generation moved past `gen` (every CTA of the group
+// arrived).  Every wait is bounded: after `limit` polls it sets the replica's
+// status word.  Returns false, in every thread, if the status word is set (a
+// wait gave up here or in another CTA of the group).
+__device__ bool group_wait(ReplicaState* st, int nct, unsigned int gen,
+                           unsigned long long limit) {
+  __shared__ int s_ok;
   if (threadIdx.x == 0) {
     volatile unsigned int* genp = &st->bar_gen;
     volatile unsigned int* statp = &st->status;
-    int ok = 1;
     if (nct > 1) {
-      const unsigned int gen = *genp;
-      __threadfence();
-      const unsigned int arrived = atomicAdd(&st->bar_count, 1u);
-      if (arrived == (unsigned int)nct - 1) {
-        st->bar_count = 0;
-        __threadfence();
-        atomicAdd(&st->bar_gen, 1u);
-      } else {
-        unsigned long long it = 0;
-        while (*genp == gen) {
-          if (*statp) break;
-          if (++it > limit) {
-            atomicOr(&st->status, 1u);
-            break;
-          }
-          if (it > 64) __nanosleep(32);
+      unsigned long long it = 0;
+      while (*genp == gen) {
+        if (*statp) break;
+        if (++it > limit) {
+          atomicOr(&st->status, 1u);
+          break;
         }
+        if (it > 64) __nanosleep(32);
       }
       __threadfence();
     }
-    s_ok = ok && (*statp == 0);
+    s_ok = *statp == 0;
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limit) {
+  const unsigned int gen = group_arrive(st, nct);
+  return group_wait(st, nct, gen, limit);
 }
 
 // CTA sums of three counts, valid in thread 0.
@@ -210,14 +229,13 @@ __device__ __forceinline__ void group_pass(const ReplicaDesc& D, int rank, int n
   }
 }
 
-// FP64 moments of one replica's current state (moments.cuh), summed by its
-// first CTA in a fixed order and accumulated into its state block.  Kept out
-// of line: it runs once per measurement and its FP64 registers would
+// FP64 moments of one replica's current state (moments.cuh): each CTA's
+// partial sums into its slot (slot = 2 * CTA + which replica of its group).
+// Kept out of line: it runs once per measurement and its FP64 registers would
 // otherwise crowd the sweep loop.
 template <int THREADS>
-__device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState* st, int rank,
-                                             int nct, double* __restrict__ partials,
-                                             unsigned long long limit) {
+__device__ __noinline__ void measure_partials(const ReplicaDesc& D, int rank, int nct,
+                                              double* __restrict__ slot) {
   double m[kObsMoments];
 #pragma unroll
   for (int t = 0; t < kObsMoments; ++t) m[t] = 0.0;
@@ -235,18 +253,21 @@ __device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState*
   if (threadIdx.x < kObsMoments) {
     double v = 0.0;
     for (int w = 0; w < THREADS / 32; ++w) v += s_m[w][threadIdx.x];
-    partials[(size_t)blockIdx.x * kObsMoments + threadIdx.x] = v;
+    slot[threadIdx.x] = v;
   }
-  if (!group_barrier(st, nct, limit)) return false;
-  if (rank != 0) return true;
-  // The group's first CTA sums the partials, one moment per thread in CTA
-  // order.  L2 loads (the partials come from other SMs; the barrier's fences
-  // made them visible there) that the compiler may issue ahead of the adds.
+}
+
+// After the group's barrier: the group's first CTA sums the partials, one
+// moment per thread in CTA order, and accumulates e = E/N, eta = sum(s)/N and
+// S into the replica's state block.  L2 loads (the partials come from other
+// SMs; the barrier's fences made them visible there).
+__device__ __noinline__ void measure_sum(const ReplicaDesc& D, ReplicaState* st, int nct,
+                                         const double* __restrict__ first_slot) {
   __shared__ double s_tot[kObsMoments];
   if (threadIdx.x < kObsMoments) {
-    const double* col = partials + (size_t)D.cta_first * kObsMoments + threadIdx.x;
     double v = 0.0;
-    for (int c = 0; c < nct; ++c) v += __ldcg(col + (size_t)c * kObsMoments);
+    for (int c = 0; c < nct; ++c) v += __ldcg(first_slot + (size_t)c * 2 * kObsMoments +
+                                               threadIdx.x);
     s_tot[threadIdx.x] = v;
   }
   __syncthreads();
@@ -270,107 +291,200 @@ __device__ __noinline__ bool measure_replica(const ReplicaDesc& D, ReplicaState*
     st->last[1] = eta;
     st->last[2] = S;
   }
-  return true;
+  __syncthreads();
 }
 
-// All sweeps of one replica by its CTA group.  Returns false if the group's
-// status word was set (a barrier wait timed out).
-template <int THREADS>
-__device__ bool run_replica(const ReplicaDesc* __restrict__ descs,
-                            ReplicaState* __restrict__ states, int rep,
-                            double* __restrict__ partials, int nsweeps, int measure_every,
-                            int measure_from, unsigned long long limit) {
-  const ReplicaDesc& D = descs[rep];
-  ReplicaState* st = states + rep;
-  const int rank = (int)blockIdx.x - D.cta_first;
-  const int nct = D.cta_count;
-  const float n3 = (float)D.nsites;
-  double d = st->d;
-  long long step = st->step;
-  __shared__ double s_d;
+// One replica as seen by one CTA of its group: where it is in its sweeps.
+struct RepCtx {
+  const ReplicaDesc* D;
+  ReplicaState* st;
+  int rank, nct, which;  // which: 0 or 1, the replica's place in its group
+  double d;
+  long long step;
+  bool pending;          // colour-0 flips of the previous sweep still to run
+  unsigned int gen;      // generation of the last arrival at the group barrier
+  unsigned int na, nf_prev, nf;
+};
 
-  // The fused two-pass sweep of the plain kernels (sweep.cu): pass A = the
-  // previous sweep's colour-0 flips (when pending) + colour-0 director
-  // trials, pass B = colour-1 director trials + colour-1 flips, and a
-  // colour-0 flip pass F closes the sweep before a measurement and after the
-  // last sweep.  Counts: director accepts of step t in cnt[t&1], flips of
-  // step t in cnt[2 + (t&1)].
-  bool pending = false;
-  for (int s = 0; s < nsweeps; ++s, ++step) {
-    const uint32_t step32 = (uint32_t)step;
-    const int par = (int)(step & 1);
+__device__ __forceinline__ void ctx_init(RepCtx& c, const ReplicaDesc* descs,
+                                         ReplicaState* states, int rep, int which) {
+  c.D = descs + rep;
+  c.st = states + rep;
+  c.rank = (int)blockIdx.x - c.D->cta_first;
+  c.nct = c.D->cta_count;
+  c.which = which;
+  c.d = c.st->d;
+  c.step = c.st->step;
+  c.pending = false;
+  c.gen = 0;
+}
+
+// The fused two-pass sweep of the plain kernels (sweep.cu): pass A = the
+// previous sweep's colour-0 flips (when pending) + colour-0 director trials,
+// pass B = colour-1 director trials + colour-1 flips, and a colour-0 flip
+// pass F closes the sweep before a measurement and after the last sweep.
+// Counts: director accepts of step t in cnt[t&1], flips of step t in
+// cnt[2 + (t&1)].  Each phase below ends where the group must meet; the
+// caller arrives at the group barrier after it and waits before the next.
+
+template <int THREADS>
+__device__ __forceinline__ void phase_a(RepCtx& c) {
+  c.na = c.nf_prev = c.nf = 0;
+  if (c.pending)
+    group_pass<kFusedA, THREADS>(*c.D, c.rank, c.nct, (uint32_t)c.step, (float)c.d, c.na,
+                                 c.nf_prev);
+  else
+    group_pass<kFusedA0, THREADS>(*c.D, c.rank, c.nct, (uint32_t)c.step, (float)c.d, c.na,
+                                  c.nf_prev);
+}
+
+template <int THREADS>
+__device__ __forceinline__ void phase_b(RepCtx& c) {
+  group_pass<kFusedB, THREADS>(*c.D, c.rank, c.nct, (uint32_t)c.step, (float)c.d, c.na, c.nf);
+}
+
+template <int THREADS>
+__device__ __forceinline__ void phase_f(RepCtx& c) {
+  group_pass<kFusedF, THREADS>(*c.D, c.rank, c.nct, (uint32_t)c.step + 1u, (float)c.d, c.na,
+                               c.nf);
+}
+
+// The CTA's counts of the sweep into the replica's counters.
+template <int THREADS>
+__device__ __forceinline__ void phase_counts(RepCtx& c) {
+  unsigned int na = c.na, nfp = c.nf_prev, nf = c.nf;
+  cta_sum3<THREADS>(na, nfp, nf);
+  if (threadIdx.x == 0) {
+    const int par = (int)(c.step & 1);
+    if (na) atomicAdd(&c.st->cnt[par], (unsigned long long)na);
+    if (nfp) atomicAdd(&c.st->cnt[2 + (par ^ 1)], (unsigned long long)nfp);
+    if (nf) atomicAdd(&c.st->cnt[2 + par], (unsigned long long)nf);
+  }
+}
+
+// After the count barrier: every CTA of the group derives the same new d
+// from the group's count (chll_mod.f90:83-90).  The counters read here are
+// reset by the group's first CTA for their next use, which no CTA reaches
+// before it passes the next barrier.
+__device__ __forceinline__ void phase_d(RepCtx& c, bool flush) {
+  __shared__ double s_d[2];
+  if (threadIdx.x == 0) {
+    ReplicaState* st = c.st;
+    const int par = (int)(c.step & 1);
+    const float n3 = (float)c.D->nsites;
+    const unsigned long long na_all = *((volatile unsigned long long*)&st->cnt[par]);
+    const float pa = (float)na_all / n3;
+    s_d[c.which] = (c.step < c.D->adapt_until) ? adapt_d(c.d, pa) : c.d;
+    if (c.rank == 0) {
+      st->cnt[par ^ 1] = 0;
+      st->paccept = pa;
+      if (c.pending) {  // flips of step-1 are complete (chll_mod.f90:93)
+        st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + (par ^ 1)]) / n3;
+        st->cnt[2 + (par ^ 1)] = 0;
+      }
+      if (flush) {
+        st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + par]) / n3;
+        st->cnt[2 + par] = 0;
+      }
+    }
+  }
+  __syncthreads();
+  c.d = s_d[c.which];
+  c.pending = !flush;
+  ++c.step;
+}
+
+// All sweeps of the one or two replicas of this CTA's group.  With two, the
+// CTA alternates them phase by phase: after arriving at one replica's group
+// barrier it runs the other replica's phase, and only then waits, so a wait
+// for the group's slowest CTA overlaps useful work.  Each replica follows
+// exactly the chain it follows alone.  Returns false if a group's status
+// word was set (a barrier wait gave up).
+template <int THREADS>
+__device__ bool run_group(const ReplicaDesc* __restrict__ descs,
+                          ReplicaState* __restrict__ states, int2 reps,
+                          double* __restrict__ partials, int nsweeps, int measure_every,
+                          int measure_from, unsigned long long limit) {
+  RepCtx c[2];
+  const int nrep = reps.y >= 0 ? 2 : 1;
+  ctx_init(c[0], descs, states, reps.x, 0);
+  if (nrep == 2) ctx_init(c[1], descs, states, reps.y, 1);
+#define CHLL_EACH(body)                 \
+  for (int r = 0; r < nrep; ++r) {      \
+    RepCtx& x = c[r];                   \
+    body;                               \
+  }
+#define CHLL_WAIT() \
+  if (!group_wait(x.st, x.nct, x.gen, limit)) return false
+#define CHLL_ARRIVE() x.gen = group_arrive(x.st, x.nct)
+  for (int s = 0; s < nsweeps; ++s) {
     const int done = s + 1;
     const bool measure =
         measure_every > 0 && done >= measure_from && done % measure_every == 0;
     const bool flush = measure || done == nsweeps;
-    unsigned int na = 0, nf_prev = 0, nf = 0;
-    if (pending)
-      group_pass<kFusedA, THREADS>(D, rank, nct, step32, (float)d, na, nf_prev);
-    else
-      group_pass<kFusedA0, THREADS>(D, rank, nct, step32, (float)d, na, nf_prev);
-    if (!group_barrier(st, nct, limit)) return false;
-    group_pass<kFusedB, THREADS>(D, rank, nct, step32, (float)d, na, nf);
+    CHLL_EACH({
+      phase_a<THREADS>(x);
+      CHLL_ARRIVE();
+    });
+    CHLL_EACH({
+      CHLL_WAIT();
+      phase_b<THREADS>(x);
+      if (!flush) phase_counts<THREADS>(x);
+      CHLL_ARRIVE();
+    });
     if (flush) {
-      if (!group_barrier(st, nct, limit)) return false;
-      group_pass<kFusedF, THREADS>(D, rank, nct, step32 + 1u, (float)d, na, nf);
+      CHLL_EACH({
+        CHLL_WAIT();
+        phase_f<THREADS>(x);
+        phase_counts<THREADS>(x);
+        CHLL_ARRIVE();
+      });
     }
-    cta_sum3<THREADS>(na, nf_prev, nf);
-    if (threadIdx.x == 0) {
-      if (na) atomicAdd(&st->cnt[par], (unsigned long long)na);
-      if (nf_prev) atomicAdd(&st->cnt[2 + (par ^ 1)], (unsigned long long)nf_prev);
-      if (nf) atomicAdd(&st->cnt[2 + par], (unsigned long long)nf);
-    }
-    if (!group_barrier(st, nct, limit)) return false;
-    // Every CTA of the group derives the same new d from the group's count
-    // (chll_mod.f90:83-90).  The counters read here are reset by the group's
-    // first CTA for their next use, which no CTA reaches before it passes the
-    // next barrier.
-    if (threadIdx.x == 0) {
-      const unsigned long long na_all = *((volatile unsigned long long*)&st->cnt[par]);
-      const float pa = (float)na_all / n3;
-      s_d = (step < D.adapt_until) ? adapt_d(d, pa) : d;
-      if (rank == 0) {
-        st->cnt[par ^ 1] = 0;
-        st->paccept = pa;
-        if (pending) {  // flips of step-1 are complete (chll_mod.f90:93)
-          st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + (par ^ 1)]) / n3;
-          st->cnt[2 + (par ^ 1)] = 0;
-        }
-        if (flush) {
-          st->faccept = (float)*((volatile unsigned long long*)&st->cnt[2 + par]) / n3;
-          st->cnt[2 + par] = 0;
-        }
+    CHLL_EACH({
+      CHLL_WAIT();
+      phase_d(x, flush);
+      if (measure) {  // FP64 measurement of the completed sweep
+        measure_partials<THREADS>(*x.D, x.rank, x.nct,
+                                  partials + ((size_t)blockIdx.x * 2 + x.which) * kObsMoments);
+        CHLL_ARRIVE();
       }
+    });
+    if (measure) {
+      CHLL_EACH({
+        CHLL_WAIT();
+        if (x.rank == 0)
+          measure_sum(*x.D, x.st, x.nct,
+                      partials + ((size_t)x.D->cta_first * 2 + x.which) * kObsMoments);
+      });
     }
-    __syncthreads();
-    d = s_d;
-    pending = !flush;
-
-    // FP64 measurement of the completed sweep
-    if (measure)
-      if (!measure_replica<THREADS>(D, st, rank, nct, partials, limit)) return false;
   }
-  if (rank == 0 && threadIdx.x == 0) {
-    st->d = d;
-    st->step = step;
-  }
+#undef CHLL_EACH
+#undef CHLL_WAIT
+#undef CHLL_ARRIVE
+  if (threadIdx.x == 0)
+    for (int r = 0; r < nrep; ++r)
+      if (c[r].rank == 0) {
+        c[r].st->d = c[r].d;
+        c[r].st->step = c[r].step;
+      }
   return true;
 }
 
 // The persistent launch walks the waves in order: in wave w, CTA b works on
-// replica cta_map[w * gridDim.x + b] (-1: idle in this wave).  Waves hold
-// replicas whose state together fits in L2, so each wave's sweeps run from
-// L2; CTAs move to their next wave as soon as their replica is done.
+// the group cta_map[w * gridDim.x + b] = {replica, second replica or -1}
+// ({-1, -1}: idle in this wave).  Waves hold replicas whose state together
+// fits the wave size, so each wave's sweeps can run from L2; CTAs move to
+// their next wave as soon as their group is done.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS)
     batch_kernel(const ReplicaDesc* __restrict__ descs, ReplicaState* __restrict__ states,
-                 const int* __restrict__ cta_map, int nwaves, double* __restrict__ partials,
+                 const int2* __restrict__ cta_map, int nwaves, double* __restrict__ partials,
                  int nsweeps, int measure_every, int measure_from, unsigned long long limit) {
   for (int w = 0; w < nwaves; ++w) {
-    const int rep = cta_map[(size_t)w * gridDim.x + blockIdx.x];
-    if (rep < 0) continue;
-    if (!run_replica<THREADS>(descs, states, rep, partials, nsweeps, measure_every,
-                              measure_from, limit))
+    const int2 reps = cta_map[(size_t)w * gridDim.x + blockIdx.x];
+    if (reps.x < 0) continue;
+    if (!run_group<THREADS>(descs, states, reps, partials, nsweeps, measure_every,
+                            measure_from, limit))
       return;
   }
 }
@@ -384,7 +498,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS)
 namespace chll {
 namespace {
 
-using BatchKernel = void (*)(const ReplicaDesc*, ReplicaState*, const int*, int, double*, int,
+using BatchKernel = void (*)(const ReplicaDesc*, ReplicaState*, const int2*, int, double*, int,
                              int, int, unsigned long long);
 
 BatchKernel kernel_for(int threads) {
@@ -427,7 +541,7 @@ struct chll_batch {
   size_t slots = 0;
   chll::ReplicaDesc* d_desc = nullptr;
   chll::ReplicaState* d_state = nullptr;
-  int* d_cta_replica = nullptr;
+  int2* d_cta_replica = nullptr;  // per wave and CTA: its group's replicas
   double* d_partials = nullptr;
   void* staging = nullptr;
   size_t staging_bytes = 0;
@@ -441,12 +555,15 @@ struct chll_batch {
   int shape_threads = -1, shape_ctas = -1;
   long long wave_bytes = 0;  // state per wave (0: all replicas in one wave)
   long long shape_wave_bytes = -1;
+  int pair = 1;  // groups of two replicas that alternate their passes (0: one replica each)
+  int shape_pair = -1;
   int nwaves = 1;
   cudaGraphExec_t graph = nullptr;
   int g_sweeps = -1, g_every = -1, g_from = -1, g_grid = -1, g_threads = -1;
   long long g_waves = -1;
   unsigned long long limit = 1ull << 24;  // polls of a group-barrier wait before it gives up
   unsigned long long g_limit = 0;
+  int g_pair = -1;
   long long total_sites = 0;
 
   chll::LatticeView view(int r) const { return desc[r].L; }
@@ -487,7 +604,7 @@ double pass_cost(const chll::ReplicaDesc& D, uint32_t threads, uint32_t* seg) {
 // per-wave CTA map (-1: idle).
 int shape_launch(chll_batch* B) {
   if (B->shape_threads == B->threads && B->shape_ctas == B->ctas_per_sm &&
-      B->shape_wave_bytes == B->wave_bytes && B->grid > 0)
+      B->shape_wave_bytes == B->wave_bytes && B->shape_pair == B->pair && B->grid > 0)
     return CHLL_OK;
   const int occ = occupancy_of(B->threads);
   if (occ <= 0) return fail(CHLL_ECUDA, "batch: kernel with %d threads cannot run", B->threads);
@@ -523,20 +640,31 @@ int shape_launch(chll_batch* B) {
       wave_load.push_back(bytes);
     }
   }
-  std::vector<int> map((size_t)waves.size() * budget, -1);
+  std::vector<int2> map((size_t)waves.size() * budget, make_int2(-1, -1));
   for (size_t w = 0; w < waves.size(); ++w) {
+    // groups of one or, paired, two replicas of neighbouring sizes (the wave
+    // is ordered largest first)
     const std::vector<int>& reps = waves[w];
-    const int n = (int)reps.size();
+    std::vector<int2> groups;
+    const int step = B->pair ? 2 : 1;
+    for (size_t t = 0; t < reps.size(); t += step)
+      groups.push_back(make_int2(reps[t], t + 1 < reps.size() && B->pair ? reps[t + 1] : -1));
+    const int n = (int)groups.size();
+    auto units = [&](int2 g) {
+      return (double)B->desc[g.x].G.units + (g.y >= 0 ? (double)B->desc[g.y].G.units : 0.0);
+    };
     double tot = 0.0;
-    for (int r : reps) tot += (double)B->desc[r].G.units;
+    for (const int2& g : groups) tot += units(g);
     std::vector<int> cnt(n, 1), cap(n);
-    for (int t = 0; t < n; ++t)
-      cap[t] = std::max(1, (int)((B->desc[reps[t]].G.units + B->threads - 1) / B->threads));
+    for (int t = 0; t < n; ++t) {
+      const uint32_t u = B->desc[groups[t].x].G.units;  // the larger replica of the group
+      cap[t] = std::max(1, (int)((u + B->threads - 1) / B->threads));
+    }
     int used = n;
     const int extra = budget - n;
     std::vector<std::pair<double, int>> rem;
     for (int t = 0; t < n; ++t) {
-      const double want = extra * (double)B->desc[reps[t]].G.units / tot;
+      const double want = extra * units(groups[t]) / tot;
       const int add = std::min((int)want, cap[t] - 1);
       cnt[t] += add;
       used += add;
@@ -552,22 +680,25 @@ int shape_launch(chll_batch* B) {
     }
     int next = 0;
     for (int t = 0; t < n; ++t) {
-      chll::ReplicaDesc& D = B->desc[reps[t]];
-      uint32_t seg = 0;
-      pass_cost(D, (uint32_t)(cnt[t] * B->threads), &seg);
-      D.W = chll::make_walk(D.G, D.L, seg ? seg : 1);
-      if (!seg) D.W.seg = 0;
-      B->desc[reps[t]].cta_first = next;
-      B->desc[reps[t]].cta_count = cnt[t];
-      for (int c = 0; c < cnt[t]; ++c) map[w * (size_t)budget + next++] = reps[t];
+      for (int r : {groups[t].x, groups[t].y}) {
+        if (r < 0) continue;
+        chll::ReplicaDesc& D = B->desc[r];
+        uint32_t seg = 0;
+        pass_cost(D, (uint32_t)(cnt[t] * B->threads), &seg);
+        D.W = chll::make_walk(D.G, D.L, seg ? seg : 1);
+        if (!seg) D.W.seg = 0;
+        D.cta_first = next;
+        D.cta_count = cnt[t];
+      }
+      for (int c = 0; c < cnt[t]; ++c) map[w * (size_t)budget + next++] = groups[t];
     }
   }
   B->grid = budget;
   B->nwaves = (int)waves.size();
   if (B->d_cta_replica) cudaFree(B->d_cta_replica);
   B->d_cta_replica = nullptr;
-  BATCH_CUDA(cudaMalloc(&B->d_cta_replica, sizeof(int) * map.size()));
-  BATCH_CUDA(cudaMemcpyAsync(B->d_cta_replica, map.data(), sizeof(int) * map.size(),
+  BATCH_CUDA(cudaMalloc(&B->d_cta_replica, sizeof(int2) * map.size()));
+  BATCH_CUDA(cudaMemcpyAsync(B->d_cta_replica, map.data(), sizeof(int2) * map.size(),
                              cudaMemcpyHostToDevice, B->stream));
   BATCH_CUDA(cudaMemcpyAsync(B->d_desc, B->desc.data(), sizeof(chll::ReplicaDesc) * B->n,
                              cudaMemcpyHostToDevice, B->stream));
@@ -575,6 +706,7 @@ int shape_launch(chll_batch* B) {
   B->shape_threads = B->threads;
   B->shape_ctas = B->ctas_per_sm;
   B->shape_wave_bytes = B->wave_bytes;
+  B->shape_pair = B->pair;
   return CHLL_OK;
 }
 
@@ -591,7 +723,7 @@ int launch_batch(chll_batch* B, cudaStream_t s, int nsweeps, int every, int from
   cfg.numAttrs = 1;
   BATCH_CUDA(cudaLaunchKernelEx(&cfg, chll::kernel_for(B->threads),
                                 (const chll::ReplicaDesc*)B->d_desc, B->d_state,
-                                (const int*)B->d_cta_replica, B->nwaves, B->d_partials, nsweeps,
+                                (const int2*)B->d_cta_replica, B->nwaves, B->d_partials, nsweeps,
                                 every, from,
                                 B->limit));
   return CHLL_OK;
@@ -602,7 +734,7 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
   if (rc != CHLL_OK) return rc;
   if (!(B->graph && B->g_sweeps == nsweeps && B->g_every == every && B->g_from == from &&
         B->g_grid == B->grid && B->g_threads == B->threads && B->g_waves == B->wave_bytes &&
-        B->g_limit == B->limit)) {
+        B->g_limit == B->limit && B->g_pair == B->pair)) {
     if (B->graph) cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
     cudaGraph_t g = nullptr;
@@ -621,6 +753,7 @@ int run_impl(chll_batch* B, int nsweeps, int every, int from) {
     B->g_threads = B->threads;
     B->g_waves = B->wave_bytes;
     B->g_limit = B->limit;
+    B->g_pair = B->pair;
   }
   BATCH_CUDA(cudaGraphLaunch(B->graph, B->stream));
   return CHLL_OK;
@@ -706,7 +839,7 @@ int chll_batch_create(const chll_replica_spec* specs, int n, chll_batch** out) {
   if ((e = cudaMalloc(&B->d_desc, sizeof(chll::ReplicaDesc) * n))) return bail(e, "descriptors");
   if ((e = cudaMalloc(&B->d_state, sizeof(chll::ReplicaState) * n))) return bail(e, "states");
   if ((e = cudaMalloc(&B->d_partials,
-                      sizeof(double) * chll::kObsMoments * B->sms * chll::kMaxCtasPerSm)))
+                      sizeof(double) * chll::kObsMoments * B->sms * chll::kMaxCtasPerSm * 2)))
     return bail(e, "partials");
   B->desc.resize(n);
   std::vector<chll::ReplicaState> st(n);
@@ -879,6 +1012,19 @@ int chll_batch_set_wait_limit(chll_batch* B, uint64_t polls) {
   return chll::record_ok();
 }
 
+int chll_batch_set_pairing(chll_batch* B, int pair) {
+  if (!B || (pair != 0 && pair != 1))
+    return fail(CHLL_EINVAL, "batch_set_pairing: pair must be 0 or 1");
+  B->pair = pair;
+  return chll::record_ok();
+}
+
+int chll_batch_get_pairing(chll_batch* B, int* pair) {
+  if (!B || !pair) return fail(CHLL_EINVAL, "batch_get_pairing: null argument");
+  *pair = B->pair;
+  return chll::record_ok();
+}
+
 int chll_batch_set_wave_bytes(chll_batch* B, int64_t wave_bytes) {
   if (!B || wave_bytes < 0) return fail(CHLL_EINVAL, "batch_set_wave_bytes: bad argument");
   B->wave_bytes = wave_bytes;
@@ -925,13 +1071,13 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
                              cudaMemcpyDeviceToDevice, B->stream));
   BATCH_CUDA(cudaMemcpyAsync(B->snap_state, B->d_state, sizeof(chll::ReplicaState) * B->n,
                              cudaMemcpyDeviceToDevice, B->stream));
-  const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm;
+  const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm, keep_pair = B->pair;
   const long long keep_waves = B->wave_bytes;
   cudaEvent_t e0, e1;
   BATCH_CUDA(cudaEventCreate(&e0));
   BATCH_CUDA(cudaEventCreate(&e1));
   double best = 1e300;
-  int bt = keep_threads, bc = keep_ctas;
+  int bt = keep_threads, bc = keep_ctas, bp = keep_pair;
   int rc = CHLL_OK;
   long long bw = B->wave_bytes;
   // Candidates: one wave, or waves of 40, 64 or 96 MiB of state (a wave that
@@ -940,6 +1086,7 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
   // occupancies (lower occupancies were never faster on this kernel).  Trials
   // measure every 10 sweeps like a production run.
   const long long kWaveOptions[] = {0ll, 40ll << 20, 64ll << 20, 96ll << 20};
+  for (int pair : {1, 0})
   for (long long wb : kWaveOptions)
   for (int threads : {128, 256, 512}) {
     const int occ = occupancy_of(threads);
@@ -948,6 +1095,7 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
       B->threads = threads;
       B->ctas_per_sm = c;
       B->wave_bytes = wb;
+      B->pair = pair;
       rc = shape_launch(B);
       if (rc != CHLL_OK) break;
       cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
@@ -968,13 +1116,16 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       if (std::getenv("CHLL_TUNE_VERBOSE"))
-        std::fprintf(stderr, "chll batch tune: threads %d ctas/SM %d wave %lld MiB waves %d: %.3f ms\n",
-                     threads, c, wb >> 20, B->nwaves, ms);
+        std::fprintf(stderr,
+                     "chll batch tune: pairs %d threads %d ctas/SM %d wave %lld MiB waves %d: "
+                     "%.3f ms\n",
+                     pair, threads, c, wb >> 20, B->nwaves, ms);
       if (ms < best) {
         best = ms;
         bt = threads;
         bc = c;
         bw = wb;
+        bp = pair;
       }
     }
   }
@@ -989,11 +1140,13 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
     B->threads = keep_threads;
     B->ctas_per_sm = keep_ctas;
     B->wave_bytes = keep_waves;
+    B->pair = keep_pair;
     return rc;
   }
   B->threads = bt;
   B->ctas_per_sm = bc;
   B->wave_bytes = bw;
+  B->pair = bp;
   if (best_threads) *best_threads = bt;
   if (best_ctas) *best_ctas = bc;
   if (best_ms) *best_ms = best;

@@ -250,6 +250,13 @@ int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
  * (0, the default: all replicas in one wave), largest first; each wave gets
  * the whole co-resident grid, in the same launch. */
 int chll_batch_set_wave_bytes(chll_batch* b, int64_t wave_bytes);
+/* pair = 1 (the default): the replicas of a wave are grouped two by two, by
+ * size, and each group's CTAs alternate the two replicas' passes, so a wait
+ * at one replica's group barrier overlaps the other replica's pass; 0: one
+ * replica per group.  The chains are the same either way.  No counterpart in
+ * the reference, which has no batched launch. */
+int chll_batch_set_pairing(chll_batch* b, int pair);
+int chll_batch_get_pairing(chll_batch* b, int* pair);
 /* How many polls a replica group's barrier wait makes before it gives up
  * (default 2^24, seconds of waiting; >= 1).  A wait that gives up sets the
  * replica's status word (column 15 of its chll_batch_moments row); every CTA

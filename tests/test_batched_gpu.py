@@ -25,17 +25,21 @@ def _specs():
     ]
 
 
-@pytest.mark.parametrize("threads,wave_bytes", [(128, 0), (256, 1), (512, 48 << 20),
-                                                (128, 64 << 10)])
-def test_batch_replicas_equal_plain_runs(threads, wave_bytes):
-    """Any launch shape and wave split gives every replica its plain chain."""
+@pytest.mark.parametrize("threads,wave_bytes,paired", [(128, 0, True), (128, 0, False),
+                                                       (256, 1, True), (512, 48 << 20, True),
+                                                       (128, 64 << 10, True),
+                                                       (256, 64 << 10, False)])
+def test_batch_replicas_equal_plain_runs(threads, wave_bytes, paired):
+    """Any launch shape, wave split and grouping (two replicas alternating
+    their passes, or one) gives every replica its plain chain."""
     from chllmodel_b200.batched import Batch
     from chllmodel_b200.lattice import Lattice, coupling
 
     specs = _specs()
     nsw = 13
     with Batch(specs) as b:
-        b.set_tuning(threads, 0, wave_bytes)
+        b.set_tuning(threads, 0, wave_bytes, paired)
+        assert b.tuning()["paired"] == paired
         if wave_bytes == 1:
             assert b.tuning()["waves"] == len(specs)  # every replica its own wave
         if wave_bytes == 64 << 10:
@@ -147,7 +151,7 @@ def test_batch_barrier_wait_gives_up():
     specs = [replica(64, kT=0.5, K=1.0, seed=3, replica=0),
              replica(8, kT=0.5, K=1.0, seed=4, replica=1)]
     with Batch(specs) as b:
-        b.set_tuning(128, 0)
+        b.set_tuning(128, 0, paired=False)  # each replica its own group
         assert b.info()["grid"] > 2  # the 64^3 replica spans many CTAs
         b.init_random()
         b.set_wait_limit(1)
