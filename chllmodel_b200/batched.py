@@ -140,7 +140,7 @@ class Batch:
     def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None, paired=None):
         """Launch shape (threads per CTA, CTAs per SM; 0: all that fit), wave
         size in bytes of state (0: one wave) and whether replica groups hold
-        two replicas that alternate their passes (the default) or one."""
+        two replicas that alternate their passes or one (the default)."""
         check(self._L.chll_batch_set_tuning(self._h, int(threads), int(ctas_per_sm)))
         if wave_bytes is not None:
             check(self._L.chll_batch_set_wave_bytes(self._h, int(wave_bytes)))

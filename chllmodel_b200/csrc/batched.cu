@@ -555,7 +555,7 @@ struct chll_batch {
   int shape_threads = -1, shape_ctas = -1;
   long long wave_bytes = 0;  // state per wave (0: all replicas in one wave)
   long long shape_wave_bytes = -1;
-  int pair = 1;  // groups of two replicas that alternate their passes (0: one replica each)
+  int pair = 0;  // 1: groups of two replicas that alternate their passes (0: one replica each)
   int shape_pair = -1;
   int nwaves = 1;
   cudaGraphExec_t graph = nullptr;

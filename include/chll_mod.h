@@ -250,11 +250,12 @@ int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
  * (0, the default: all replicas in one wave), largest first; each wave gets
  * the whole co-resident grid, in the same launch. */
 int chll_batch_set_wave_bytes(chll_batch* b, int64_t wave_bytes);
-/* pair = 1 (the default): the replicas of a wave are grouped two by two, by
- * size, and each group's CTAs alternate the two replicas' passes, so a wait
- * at one replica's group barrier overlaps the other replica's pass; 0: one
- * replica per group.  The chains are the same either way.  No counterpart in
- * the reference, which has no batched launch. */
+/* pair = 1: the replicas of a wave are grouped two by two, by size, and each
+ * group's CTAs alternate the two replicas' passes, so a wait at one
+ * replica's group barrier overlaps the other replica's pass; 0 (the
+ * default): one replica per group.  The chains are the same either way;
+ * chll_batch_autotune tries both.  No counterpart in the reference, which
+ * has no batched launch. */
 int chll_batch_set_pairing(chll_batch* b, int pair);
 int chll_batch_get_pairing(chll_batch* b, int* pair);
 /* How many polls a replica group's barrier wait makes before it gives up
