@@ -51,10 +51,10 @@ BATCH_NOUT = 50
 BYTES_PER_SITE_PASS = 24  # 16 B read (every site once) + 8 B written (half the sites)
 # ncu figures of the fused pass kernels A and B on the 480^3 benchmark lattice
 # (one capture of two launches, mean of A and B; profiles/fused_pass_kernel_480cube_metrics.md):
-# DRAM bytes read + written per site and launch (A 2647.6 MB, B 2652.6 MB
+# DRAM bytes read + written per site and launch (A 2653.0 MB, B 2651.2 MB
 # for 110.6 M sites), and warp-level instructions x 32 per updated site
-# (A 340.6 M, B 372.6 M warp instructions; a launch updates half the sites).
-PASS_PROFILE = {"traffic_bytes_per_site": 23.96, "thread_instr_per_updated_site": 206.4,
+# (A 344.8 M, B 339.6 M warp instructions; a launch updates half the sites).
+PASS_PROFILE = {"traffic_bytes_per_site": 23.98, "thread_instr_per_updated_site": 198.0,
                 "source": "ncu dram__bytes_read+write at 480^3"}
 METRIC = "site_updates_per_s"
 UNIT = "site-updates/s"
