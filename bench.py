@@ -472,7 +472,14 @@ def gpu_arm(args):
                 "(Philox seed 11 + rank); state FP32, observables FP64",
         "config": {"workload": _workload(edge), "lattice": [edge, edge, edge],
                    "boundary": "periodic", "kT": KT, "K": KK, "h": FIELD, "eps": EPS,
-                   "d0": D0, "nout": NOUT, "parallelism": f"replicas x{world}",
+                   "d0": D0, "nout": NOUT,
+                   "measurements_in_timed_region": sum(
+                       1 for t in range(step0, step0 + args.steps) if t % NOUT == 0),
+                   "measurement_note": f"a measurement every {NOUT} sweeps, counted by sweep "
+                                       f"number: a region of fewer sweeps may hold none; the "
+                                       f"e2e leg's {max(args.e2e_sweeps, NOUT)} sweeps hold "
+                                       f"their share",
+                   "parallelism": f"replicas x{world}",
                    "l2": f"lattice {16 * n / 1e9:.2f} GB vs 126 MB L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak,
