@@ -15,6 +15,11 @@ and committed, and nothing at test time reads the reference tree.
    (the stencil fixes KK = 1.0 and has no field term).
 2. ``philox_kat.json`` -- the published Philox4x32-10 known-answer vectors
    (Salmon et al., SC'11, Random123 distribution).
+4. ``chi_golden.npz`` -- the reference's own measure_chi
+   (notebooks/.ipynb_checkpoints/Xch-checkpoint.ipynb, cell 2: chiral
+   susceptibility, mean enantiomeric excess and specific heat from the macro
+   CSV files) run on seeded CSV files in ChLLSim's format, its matplotlib
+   calls recorded instead of drawn.
 3. ``analysis_golden.npz`` -- the reference's own analysis functions run on
    small seeded fields: calc_n_corr / calc_s_corr (notebooks/paper_plots2.ipynb,
    cell 0) and structure_factor / get_sc
@@ -155,6 +160,79 @@ def make_analysis_fixture(path):
     np.savez_compressed(path, **out)
 
 
+class _Recorder:
+    """Stands in for matplotlib: every call returns itself, and the scatter()
+    calls' arguments are kept (measure_chi plots its results)."""
+
+    def __init__(self):
+        self.scatters = []
+
+    def subplots(self, *a, **k):
+        return self, (self, self, self)
+
+    def scatter(self, x, y, *a, **k):
+        self.scatters.append((list(x), list(y)))
+
+    def __getattr__(self, name):
+        return lambda *a, **k: self
+
+
+def make_chi_fixture(path):
+    """The reference's measure_chi (notebooks/.ipynb_checkpoints/
+    Xch-checkpoint.ipynb, cell 2: chiral susceptibility, mean excess and
+    specific heat from the macro CSVs) run on seeded CSVs written in
+    ChLLSim's format (Step,TotalEnergy,Eexcess,Paccept,Faccept,D), with
+    load_csv from cell 0."""
+    import tempfile
+
+    nb = json.load(open(os.path.join(REF, "notebooks", ".ipynb_checkpoints",
+                                     "Xch-checkpoint.ipynb")))
+    cell0 = "".join(nb["cells"][0]["source"])
+    cell2 = "".join(nb["cells"][2]["source"])
+    load_src = cell0[cell0.index("def load_csv"):cell0.index("def plot_energy")]
+    chi_src = cell2[cell2.index("def measure_chi"):cell2.index("measure_chi(0.001)")]
+    rng = np.random.default_rng(20251204)
+    points = [(1.0, 0.3), (1.0, 0.7), (1.0, 1.3), (0.1, 0.5)]
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "nb"))
+        files = []
+        for q, (K, kbt) in enumerate(points):
+            name = f"aligned_K{K}_kbt{kbt}"
+            os.makedirs(os.path.join(tmp, "data", name))
+            rows = np.column_stack([
+                np.arange(1, 201) * 50,
+                rng.normal(-1.5, 0.02, 200),        # TotalEnergy (per site)
+                rng.normal(0.1 * q, 0.05, 200),     # Eexcess
+                rng.uniform(0.3, 0.7, 200), rng.uniform(0.3, 0.7, 200),
+                rng.uniform(0.05, 0.2, 200)])
+            rel = f"../data/{name}/{name}.csv"
+            with open(os.path.join(tmp, "data", name, f"{name}.csv"), "w") as f:
+                f.write("Step,TotalEnergy,Eexcess,Paccept,Faccept,D\n")
+                for r in rows:
+                    f.write(f"{int(r[0])}," + ",".join(repr(float(v)) for v in r[1:]) + "\n")
+            files.append(rel)
+            out[f"p{q}_rows"] = rows
+        cwd = os.getcwd()
+        os.chdir(os.path.join(tmp, "nb"))
+        try:
+            rec = _Recorder()
+            ns = {"np": np, "plt": rec, "csvfiles": sorted(files)}
+            exec(load_src + chi_src, ns)
+            for K in sorted({p[0] for p in points}):
+                rec.scatters = []
+                ns["measure_chi"](K)
+                (kbts, chi), (_, ent), (_, cv) = rec.scatters
+                out[f"K{K}_kbts"] = np.asarray(kbts)
+                out[f"K{K}_chi"] = np.asarray(chi)
+                out[f"K{K}_excess"] = np.asarray(ent)
+                out[f"K{K}_cv"] = np.asarray(cv)
+        finally:
+            os.chdir(cwd)
+    out["points"] = np.asarray(points)
+    np.savez_compressed(path, **out)
+
+
 def main():
     global REF
     import argparse
@@ -167,6 +245,7 @@ def main():
         ap.error("give --reference PATH (or CHLL_REFERENCE_TREE): a ChLLModel checkout")
     make_ekernel_fixture(os.path.join(HERE, "ekernel_energy.npz"))
     make_analysis_fixture(os.path.join(HERE, "analysis_golden.npz"))
+    make_chi_fixture(os.path.join(HERE, "chi_golden.npz"))
     with open(os.path.join(HERE, "philox_kat.json"), "w") as f:
         json.dump({"generator": "philox4x32-10", "vectors": PHILOX_KAT}, f, indent=1)
     print("wrote", os.listdir(HERE))

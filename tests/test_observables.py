@@ -68,3 +68,43 @@ def test_phase_grid_is_the_batched_config():
     assert sorted({round(s["g"], 6) for s in specs}) == [round(x, 6) for x in gs]
     assert phase_grid(kTs, gs, [32, 48, 64], seed=1) == specs
     assert all(math.isclose(s["K"], 1.0) and s["boundary"] == "periodic" for s in specs)
+
+
+def test_fluctuations_match_the_reference_measure_chi(golden_dir, tmp_path):
+    """chll.ChLLSim writes the reference's macro CSV (Step,TotalEnergy,
+    Eexcess,Paccept,Faccept,D); the reference's measure_chi
+    (notebooks/.ipynb_checkpoints/Xch-checkpoint.ipynb, cell 2) read seeded
+    files of that format (tests/golden/chi_golden.npz, generated by running it).
+    The fluctuation formulas of chllmodel_b200.observables in their reference
+    forms give its numbers, and a file written by save_macros reads back to
+    the rows it holds."""
+    import os
+
+    import numpy as np
+
+    from chllmodel_b200 import chll
+    from chllmodel_b200 import observables as ob
+
+    d = np.load(os.path.join(golden_dir, "chi_golden.npz"))
+    pts = [tuple(p) for p in d["points"]]
+    for K in sorted({p[0] for p in pts}):
+        got_chi, got_ex, got_cv = [], [], []
+        for q, (k, kbt) in enumerate(pts):
+            if k != K:
+                continue
+            rows = d[f"p{q}_rows"]
+            got_chi.append(ob.chiral_susceptibility(rows[:, 2], kbt, 1, reference_form=False))
+            got_ex.append(float(np.mean(rows[:, 2])))
+            got_cv.append(ob.specific_heat_reference(rows[:, 1], kbt))
+        np.testing.assert_allclose(got_chi, d[f"K{K}_chi"], rtol=1e-12)
+        np.testing.assert_allclose(got_ex, d[f"K{K}_excess"], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(got_cv, d[f"K{K}_cv"], rtol=1e-12)
+    # the CSV that ChLLSim writes is the file measure_chi reads
+    sim = chll.ChLLSim(4, 4, 4, 0.5, 0.1, 1.0, 0.0, 0.0, name="csvcheck", overwrite=True,
+                       verbose=False, data_folder=str(tmp_path))
+    rows = d["p0_rows"]
+    sim.msteps = rows[:, 0].astype(np.int32)
+    sim.m = np.asfortranarray(rows[:, 1:6])
+    sim.save_macros()
+    back = np.loadtxt(os.path.join(sim.simpath, "csvcheck.csv"), skiprows=1, delimiter=",")
+    np.testing.assert_array_equal(back, rows)
