@@ -674,9 +674,11 @@ def batched_vs_plain(args, rank, torch):
     if args.batched_shape:
         t, c = (int(x) for x in args.batched_shape.split("x"))
         paired = None if args.batched_pairs < 0 else bool(args.batched_pairs)
-        b.set_tuning(t, c, args.batched_wave_mb << 20, paired)
+        pooled = None if args.batched_pooled < 0 else bool(args.batched_pooled)
+        b.set_tuning(t, c, args.batched_wave_mb << 20, paired, pooled)
         tune = {"threads": t, "ctas_per_sm": c, "wave_bytes": args.batched_wave_mb << 20,
-                "paired": b.tuning()["paired"], "trial_ms": None}
+                "paired": b.tuning()["paired"], "pooled": b.tuning()["pooled"],
+                "trial_ms": None}
     else:
         tune = b.autotune(trial_sweeps=200)
     b.run(nsw, measure_every=BATCH_NOUT)   # warm-up: graph capture and first launch
@@ -685,7 +687,8 @@ def batched_vs_plain(args, rank, torch):
     b = Batch(specs)
     b.set_stream(stream.cuda_stream)
     b.init_random()
-    b.set_tuning(tune["threads"], tune["ctas_per_sm"], tune["wave_bytes"], tune["paired"])
+    b.set_tuning(tune["threads"], tune["ctas_per_sm"], tune["wave_bytes"], tune["paired"],
+                 tune["pooled"])
     b.sync()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -747,7 +750,8 @@ def batched_vs_plain(args, rank, torch):
             "sequential_chllsim_s": t_sim,
             "speedup_vs_sequential_chllsim": t_sim / t_batched,
             "site_updates_per_s": total * nsw / t_batched,
-            "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "paired", "trial_ms")},
+            "tuning": dict({k: tune[k] for k in ("threads", "ctas_per_sm", "paired", "pooled",
+                                                 "trial_ms")},
                            **{"waves": info_tune["waves"],
                               "wave_MiB": info_tune["wave_bytes"] / 2 ** 20}),
             "grid_ctas": info["grid"],
@@ -863,6 +867,9 @@ def main():
                     help="THREADSxCTAS_PER_SM for the batched launch instead of autotuning")
     ap.add_argument("--batched-wave-mb", type=int, default=0,
                     help="wave size with --batched-shape (0: all replicas in one wave)")
+    ap.add_argument("--batched-pooled", type=int, default=-1,
+                    help="with --batched-shape: 1 pooled passes, 0 the persistent launch "
+                         "(default: the library's)")
     ap.add_argument("--batched-pairs", type=int, default=-1,
                     help="with --batched-shape: 1 replica groups of two alternating replicas, "
                          "0 one replica per group (default: the library's)")

@@ -39,7 +39,8 @@ EXPORTS = (
     "chll_batch_init_random", "chll_batch_upload_f4", "chll_batch_download_f4", "chll_batch_run",
     "chll_batch_moments", "chll_batch_info", "chll_batch_set_tuning", "chll_batch_autotune",
     "chll_batch_set_wave_bytes", "chll_batch_get_tuning", "chll_batch_set_wait_limit",
-    "chll_batch_set_pairing", "chll_batch_get_pairing",
+    "chll_batch_set_pairing", "chll_batch_get_pairing", "chll_batch_set_pooled",
+    "chll_batch_get_pooled",
 )
 
 
@@ -207,12 +208,15 @@ def _declare(L: ct.CDLL) -> None:
     L.chll_batch_set_wait_limit.argtypes = [vp, ct.c_uint64]
     L.chll_batch_set_pairing.argtypes = [vp, i32]
     L.chll_batch_get_pairing.argtypes = [vp, P(i32)]
+    L.chll_batch_set_pooled.argtypes = [vp, i32]
+    L.chll_batch_get_pooled.argtypes = [vp, P(i32)]
     L.chll_batch_get_tuning.argtypes = [vp, P(ct.c_int32), P(ct.c_int32), P(i64), P(ct.c_int32)]
     for name in ("chll_batch_set_stream", "chll_batch_sync", "chll_batch_init_random",
                  "chll_batch_run", "chll_batch_moments", "chll_batch_download_f4",
                  "chll_batch_upload_f4", "chll_batch_info", "chll_batch_set_tuning",
                  "chll_batch_autotune", "chll_batch_set_wave_bytes", "chll_batch_get_tuning",
-                 "chll_batch_set_wait_limit", "chll_batch_set_pairing", "chll_batch_get_pairing"):
+                 "chll_batch_set_wait_limit", "chll_batch_set_pairing", "chll_batch_get_pairing",
+                 "chll_batch_set_pooled", "chll_batch_get_pooled"):
         getattr(L, name).restype = i32
 
 

@@ -137,15 +137,19 @@ class Batch:
                                       ct.byref(g)))
         return {"total_sites": n.value, "replicas": r.value, "threads": t.value, "grid": g.value}
 
-    def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None, paired=None):
+    def set_tuning(self, threads, ctas_per_sm=0, wave_bytes=None, paired=None, pooled=None):
         """Launch shape (threads per CTA, CTAs per SM; 0: all that fit), wave
         size in bytes of state (0: one wave) and whether replica groups hold
-        two replicas that alternate their passes or one (the default)."""
+        two replicas that alternate their passes or one (the default) -- all
+        for the persistent launch -- and whether to sweep as pooled passes
+        instead (one launch per pass over all replicas)."""
         check(self._L.chll_batch_set_tuning(self._h, int(threads), int(ctas_per_sm)))
         if wave_bytes is not None:
             check(self._L.chll_batch_set_wave_bytes(self._h, int(wave_bytes)))
         if paired is not None:
             check(self._L.chll_batch_set_pairing(self._h, int(bool(paired))))
+        if pooled is not None:
+            check(self._L.chll_batch_set_pooled(self._h, int(bool(pooled))))
 
     def set_wait_limit(self, polls):
         """Polls a replica group's barrier wait makes before it gives up and
@@ -157,8 +161,10 @@ class Batch:
         check(self._L.chll_batch_get_tuning(self._h, ct.byref(t), ct.byref(c), ct.byref(w),
                                             ct.byref(n)))
         check(self._L.chll_batch_get_pairing(self._h, ct.byref(p)))
+        q = ct.c_int32()
+        check(self._L.chll_batch_get_pooled(self._h, ct.byref(q)))
         return {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": w.value,
-                "waves": n.value, "paired": bool(p.value)}
+                "waves": n.value, "paired": bool(p.value), "pooled": bool(q.value)}
 
     def autotune(self, trial_sweeps=20, cache=None) -> dict:
         """Times every launch shape on this replica set and keeps the fastest.
@@ -170,14 +176,15 @@ class Batch:
             if key in table:
                 e = table[key]
                 self.set_tuning(e["threads"], e["ctas_per_sm"], e.get("wave_bytes"),
-                                e.get("paired"))
+                                e.get("paired"), e.get("pooled"))
                 return dict(e, cached=True)
         t, c, ms = ct.c_int(), ct.c_int(), ct.c_double()
         check(self._L.chll_batch_autotune(self._h, int(trial_sweeps), ct.byref(t), ct.byref(c),
                                           ct.byref(ms)))
         tun = self.tuning()
         res = {"threads": t.value, "ctas_per_sm": c.value, "wave_bytes": tun["wave_bytes"],
-               "waves": tun["waves"], "paired": tun["paired"], "trial_ms": ms.value,
+               "waves": tun["waves"], "paired": tun["paired"], "pooled": tun["pooled"],
+               "trial_ms": ms.value,
                "trial_sweeps": int(trial_sweeps)}
         if cache:
             table = {}

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -37,6 +38,7 @@
 #include "../../include/chll_mod.h"
 #include "chll_common.cuh"
 #include "moments.cuh"
+#include "pooled.cuh"
 #include "sweep.cuh"
 #include "sweep_unit.cuh"
 
@@ -76,26 +78,6 @@ struct ReplicaState {
 
 constexpr int kMomLen = 16;  // chll_batch_moments row
 
-// Largest eigenvalue of a symmetric 3x3 matrix (Smith, "Eigenvalues of a
-// symmetric 3x3 matrix", CACM 4(4):168, 1961): trigonometric solution of the
-// characteristic cubic.
-__host__ __device__ inline double sym3_max_eig(double a11, double a22, double a33, double a12,
-                                               double a13, double a23) {
-  const double p1 = a12 * a12 + a13 * a13 + a23 * a23;
-  const double q = (a11 + a22 + a33) / 3.0;
-  const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
-  const double p2 = b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * p1;
-  if (p2 <= 0.0) return q;
-  const double p = sqrt(p2 / 6.0);
-  const double c11 = b11 / p, c22 = b22 / p, c33 = b33 / p;
-  const double c12 = a12 / p, c13 = a13 / p, c23 = a23 / p;
-  const double det = c11 * (c22 * c33 - c23 * c23) - c12 * (c12 * c33 - c23 * c13) +
-                     c13 * (c12 * c23 - c22 * c13);
-  double r = det / 2.0;
-  r = r < -1.0 ? -1.0 : (r > 1.0 ? 1.0 : r);
-  const double phi = acos(r) / 3.0;
-  return q + 2.0 * p * cos(phi);
-}
 
 // Group barrier of one replica's CTAs, split in two so that a CTA can do
 // other work between arriving and waiting (a second replica's pass).
@@ -145,11 +127,6 @@ __device__ bool group_wait(ReplicaState* st, int nct, unsigned int gen,
   }
   __syncthreads();
   return s_ok != 0;
-}
-
-__device__ bool group_barrier(ReplicaState* st, int nct, unsigned long long limit) {
-  const unsigned int gen = group_arrive(st, nct);
-  return group_wait(st, nct, gen, limit);
 }
 
 // CTA sums of three counts, valid in thread 0.
@@ -489,6 +466,31 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS)
   }
 }
 
+// Pooled mode (pooled.cu): each replica's d and step move into a plain
+// control block for the pooled passes, and back.
+__global__ void states_to_controls(const ReplicaDesc* __restrict__ descs,
+                                   const ReplicaState* __restrict__ states,
+                                   Control* __restrict__ ctl, int n) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  Control c = {};
+  c.d = states[r].d;
+  c.step = states[r].step;
+  c.adapt_until = descs[r].adapt_until;
+  c.nsites = descs[r].nsites;
+  ctl[r] = c;
+}
+
+__global__ void controls_to_states(const Control* __restrict__ ctl,
+                                   ReplicaState* __restrict__ states, int n) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  states[r].d = ctl[r].d;
+  states[r].step = ctl[r].step;
+  states[r].paccept = ctl[r].paccept;
+  states[r].faccept = ctl[r].faccept;
+}
+
 }  // namespace
 }  // namespace chll
 
@@ -559,6 +561,15 @@ struct chll_batch {
   int shape_pair = -1;
   int nwaves = 1;
   cudaGraphExec_t graph = nullptr;
+  // pooled mode (pooled.cu): one launch per pass over all replicas' units
+  int pooled = 0;
+  chll::Control* d_ctl = nullptr;
+  chll::PoolEntry* d_pool = nullptr;
+  double* d_pool_partials = nullptr;
+  uint32_t pool_units = 0, pool_units_per_cta = 0, pool_slots = 0, pool_slots_per_cta = 0;
+  int pool_grid = 0, pool_mom_grid = 0;
+  cudaGraphExec_t pool_graph[2] = {nullptr, nullptr};  // a chunk without / with a measurement
+  int pool_graph_sweeps[2] = {-1, -1};
   int g_sweeps = -1, g_every = -1, g_from = -1, g_grid = -1, g_threads = -1;
   long long g_waves = -1;
   unsigned long long limit = 1ull << 24;  // polls of a group-barrier wait before it gives up
@@ -729,7 +740,120 @@ int launch_batch(chll_batch* B, cudaStream_t s, int nsweeps, int every, int from
   return CHLL_OK;
 }
 
+// The pool's layout: replicas in order, each replica's units and storage
+// slots contiguous; equal blocks of units (pass launches) and of slots
+// (moments launches) per CTA, and for each replica the CTAs that meet it.
+int pool_prepare(chll_batch* B) {
+  if (B->d_pool) return CHLL_OK;
+  const int grid = chll::pool_pass_ctas();
+  std::vector<chll::PoolEntry> ent(B->n);
+  uint64_t units = 0, slots = 0;
+  for (int r = 0; r < B->n; ++r) {
+    ent[r].unit_begin = (uint32_t)units;
+    ent[r].slot_begin = (uint32_t)slots;
+    units += B->desc[r].G.units;
+    slots += 2ull * B->desc[r].M.per_colour;
+  }
+  if (units >= (1ull << 31) || slots >= (1ull << 32))
+    return fail(CHLL_EINVAL, "batch: pooled mode takes fewer than 2^31 units in all");
+  const uint32_t upc = (uint32_t)((units + grid - 1) / grid);
+  const uint32_t spc = (uint32_t)((slots + grid - 1) / grid);
+  B->pool_units = (uint32_t)units;
+  B->pool_slots = (uint32_t)slots;
+  B->pool_units_per_cta = std::max(upc, 1u);
+  B->pool_slots_per_cta = std::max(spc, 1u);
+  B->pool_grid = (int)((units + B->pool_units_per_cta - 1) / B->pool_units_per_cta);
+  B->pool_mom_grid = (int)((slots + B->pool_slots_per_cta - 1) / B->pool_slots_per_cta);
+  BATCH_CUDA(cudaMalloc(&B->d_ctl, sizeof(chll::Control) * B->n));
+  int partials = 0;
+  for (int r = 0; r < B->n; ++r) {
+    const chll::ReplicaDesc& D = B->desc[r];
+    chll::PoolEntry& E = ent[r];
+    E.L = D.L;
+    E.G = D.G;
+    E.M = D.M;
+    E.cp = D.cp;
+    E.cd = D.cd;
+    E.key0 = D.key0;
+    E.key1 = D.key1;
+    E.replica = D.replica;
+    E.full = D.L.ni % 4 == 0;
+    E.nsites = D.nsites;
+    const uint32_t u0 = E.unit_begin, u1 = u0 + D.G.units - 1;
+    E.pass_cta_first = (int)(u0 / B->pool_units_per_cta);
+    E.pass_ctas = (int)(u1 / B->pool_units_per_cta) - E.pass_cta_first + 1;
+    const uint32_t s0 = E.slot_begin, s1 = s0 + 2 * D.M.per_colour - 1;
+    E.mom_cta_first = (int)(s0 / B->pool_slots_per_cta);
+    E.mom_ctas = (int)(s1 / B->pool_slots_per_cta) - E.mom_cta_first + 1;
+    E.partial_first = partials;
+    partials += E.mom_ctas;
+    E.ctl = B->d_ctl + r;
+    // device addresses of the replica's accumulators (no host access)
+    char* st = reinterpret_cast<char*>(B->d_state + r);
+    E.mom = reinterpret_cast<double*>(st + offsetof(chll::ReplicaState, mom));
+    E.last = reinterpret_cast<double*>(st + offsetof(chll::ReplicaState, last));
+  }
+  BATCH_CUDA(cudaMalloc(&B->d_pool_partials, sizeof(double) * chll::kObsMoments * partials));
+  BATCH_CUDA(cudaMalloc(&B->d_pool, sizeof(chll::PoolEntry) * B->n));
+  BATCH_CUDA(cudaMemcpyAsync(B->d_pool, ent.data(), sizeof(chll::PoolEntry) * B->n,
+                             cudaMemcpyHostToDevice, B->stream));
+  BATCH_CUDA(cudaStreamSynchronize(B->stream));
+  return CHLL_OK;
+}
+
+// The launches of `sweeps` fused sweeps of every replica (A0 B (A B)... F),
+// then, with `measure`, the FP64 moments.
+void pool_chunk(chll_batch* B, cudaStream_t s, int sweeps, bool measure) {
+  auto pass = [&](int phase) {
+    chll::launch_pool_pass(B->d_pool, B->n, B->pool_units, B->pool_units_per_cta, B->pool_grid,
+                           phase, s);
+  };
+  for (int t = 0; t < sweeps; ++t) {
+    pass(t ? chll::kFusedA : chll::kFusedA0);
+    pass(chll::kFusedB);
+  }
+  pass(chll::kFusedF);
+  if (measure)
+    chll::launch_pool_moments(B->d_pool, B->n, B->pool_slots, B->pool_slots_per_cta,
+                              B->pool_mom_grid, B->d_pool_partials, s);
+}
+
+int pool_run(chll_batch* B, int nsweeps, int every, int from) {
+  int rc = pool_prepare(B);
+  if (rc != CHLL_OK) return rc;
+  chll::states_to_controls<<<(B->n + 127) / 128, 128, 0, B->stream>>>(B->d_desc, B->d_state,
+                                                                      B->d_ctl, B->n);
+  BATCH_CUDA(cudaGetLastError());
+  const int chunk = every > 0 ? every : nsweeps;
+  for (int done = 0; done < nsweeps;) {
+    const int c = std::min(chunk, nsweeps - done);
+    done += c;
+    const bool measure = every > 0 && done >= from && done % every == 0;
+    cudaGraphExec_t& ge = B->pool_graph[measure];
+    if (!ge || B->pool_graph_sweeps[measure] != c) {
+      if (ge) cudaGraphExecDestroy(ge);
+      ge = nullptr;
+      cudaGraph_t g = nullptr;
+      BATCH_CUDA(cudaStreamBeginCapture(B->capture_stream, cudaStreamCaptureModeThreadLocal));
+      pool_chunk(B, B->capture_stream, c, measure);
+      cudaError_t e = cudaStreamEndCapture(B->capture_stream, &g);
+      if (e != cudaSuccess) return fail(CHLL_ECUDA, "batch: pooled capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess)
+        return fail(CHLL_ECUDA, "batch: pooled instantiate: %s", cudaGetErrorString(e));
+      B->pool_graph_sweeps[measure] = c;
+    }
+    BATCH_CUDA(cudaGraphLaunch(ge, B->stream));
+  }
+  chll::controls_to_states<<<(B->n + 127) / 128, 128, 0, B->stream>>>(B->d_ctl, B->d_state,
+                                                                      B->n);
+  BATCH_CUDA(cudaGetLastError());
+  return CHLL_OK;
+}
+
 int run_impl(chll_batch* B, int nsweeps, int every, int from) {
+  if (B->pooled) return pool_run(B, nsweeps, every, from);
   int rc = shape_launch(B);
   if (rc != CHLL_OK) return rc;
   if (!(B->graph && B->g_sweeps == nsweeps && B->g_every == every && B->g_from == from &&
@@ -889,6 +1013,11 @@ void chll_batch_destroy(chll_batch* B) {
   if (B->own_stream) cudaStreamSynchronize(B->own_stream);
   if (B->stream && B->stream != B->own_stream) cudaStreamSynchronize(B->stream);
   if (B->graph) cudaGraphExecDestroy(B->graph);
+  for (cudaGraphExec_t g : B->pool_graph)
+    if (g) cudaGraphExecDestroy(g);
+  cudaFree(B->d_ctl);
+  cudaFree(B->d_pool);
+  cudaFree(B->d_pool_partials);
   cudaFree(B->lat);
   cudaFree(B->d_desc);
   cudaFree(B->d_state);
@@ -1012,6 +1141,19 @@ int chll_batch_set_wait_limit(chll_batch* B, uint64_t polls) {
   return chll::record_ok();
 }
 
+int chll_batch_set_pooled(chll_batch* B, int pooled) {
+  if (!B || (pooled != 0 && pooled != 1))
+    return fail(CHLL_EINVAL, "batch_set_pooled: pooled must be 0 or 1");
+  B->pooled = pooled;
+  return chll::record_ok();
+}
+
+int chll_batch_get_pooled(chll_batch* B, int* pooled) {
+  if (!B || !pooled) return fail(CHLL_EINVAL, "batch_get_pooled: null argument");
+  *pooled = B->pooled;
+  return chll::record_ok();
+}
+
 int chll_batch_set_pairing(chll_batch* B, int pair) {
   if (!B || (pair != 0 && pair != 1))
     return fail(CHLL_EINVAL, "batch_set_pairing: pair must be 0 or 1");
@@ -1071,7 +1213,9 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
                              cudaMemcpyDeviceToDevice, B->stream));
   BATCH_CUDA(cudaMemcpyAsync(B->snap_state, B->d_state, sizeof(chll::ReplicaState) * B->n,
                              cudaMemcpyDeviceToDevice, B->stream));
-  const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm, keep_pair = B->pair;
+  const int keep_threads = B->threads, keep_ctas = B->ctas_per_sm, keep_pair = B->pair,
+            keep_pooled = B->pooled;
+  B->pooled = 0;
   const long long keep_waves = B->wave_bytes;
   cudaEvent_t e0, e1;
   BATCH_CUDA(cudaEventCreate(&e0));
@@ -1129,6 +1273,38 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
       }
     }
   }
+  // the pooled passes (pooled.cu): no launch shape to choose; timed on the
+  // second of two trials (the first captures the chunk graph)
+  int bpool = 0;
+  if (rc == CHLL_OK) {
+    B->pooled = 1;
+    for (int trial = 0; trial < 2 && rc == CHLL_OK; ++trial) {
+      cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
+                      B->stream);
+      cudaMemcpyAsync(B->d_state, B->snap_state, sizeof(chll::ReplicaState) * B->n,
+                      cudaMemcpyDeviceToDevice, B->stream);
+      cudaEventRecord(e0, B->stream);
+      rc = pool_run(B, trial_sweeps, 10, 0);
+      cudaEventRecord(e1, B->stream);
+      if (rc != CHLL_OK) break;
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        rc = fail(CHLL_ECUDA, "batch_autotune: %s", cudaGetErrorString(e));
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (trial == 1) {
+        if (std::getenv("CHLL_TUNE_VERBOSE"))
+          std::fprintf(stderr, "chll batch tune: pooled passes: %.3f ms\n", ms);
+        if (ms < best) {
+          best = ms;
+          bpool = 1;
+        }
+      }
+    }
+    B->pooled = 0;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaMemcpyAsync(B->lat, B->snap_lat, B->slots * sizeof(float4), cudaMemcpyDeviceToDevice,
@@ -1141,12 +1317,14 @@ int chll_batch_autotune(chll_batch* B, int trial_sweeps, int* best_threads, int*
     B->ctas_per_sm = keep_ctas;
     B->wave_bytes = keep_waves;
     B->pair = keep_pair;
+    B->pooled = keep_pooled;
     return rc;
   }
   B->threads = bt;
   B->ctas_per_sm = bc;
   B->wave_bytes = bw;
   B->pair = bp;
+  B->pooled = bpool;
   if (best_threads) *best_threads = bt;
   if (best_ctas) *best_ctas = bc;
   if (best_ms) *best_ms = best;

@@ -9,6 +9,8 @@
 //          the diagonal neighbour (ip1,jp1,k) exactly as chll_mod.f90:438;
 //   acc[2] s;  acc[3..8] nx*nx, ny*ny, nz*nz, nx*ny, nx*nz, ny*nz.
 #pragma once
+#include <cmath>
+
 #include "chll_common.cuh"
 
 namespace chll {
@@ -118,6 +120,27 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Largest eigenvalue of a symmetric 3x3 matrix (Smith, "Eigenvalues of a
+// symmetric 3x3 matrix", CACM 4(4):168, 1961): trigonometric solution of the
+// characteristic cubic.
+__host__ __device__ inline double sym3_max_eig(double a11, double a22, double a33, double a12,
+                                               double a13, double a23) {
+  const double p1 = a12 * a12 + a13 * a13 + a23 * a23;
+  const double q = (a11 + a22 + a33) / 3.0;
+  const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
+  const double p2 = b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * p1;
+  if (p2 <= 0.0) return q;
+  const double p = sqrt(p2 / 6.0);
+  const double c11 = b11 / p, c22 = b22 / p, c33 = b33 / p;
+  const double c12 = a12 / p, c13 = a13 / p, c23 = a23 / p;
+  const double det = c11 * (c22 * c33 - c23 * c23) - c12 * (c12 * c33 - c23 * c13) +
+                     c13 * (c12 * c23 - c22 * c13);
+  double r = det / 2.0;
+  r = r < -1.0 ? -1.0 : (r > 1.0 ? 1.0 : r);
+  const double phi = acos(r) / 3.0;
+  return q + 2.0 * p * cos(phi);
 }
 
 }  // namespace chll

@@ -114,28 +114,6 @@ __global__ void __launch_bounds__(kThreads, 3)
 // Control epilogue (last CTA): B closes the director count (paccept, d) and
 // advances the step; A and F close the previous sweep's flip count
 // (faccept), which B started with the colour-1 flips.
-// The control update after a fused pass, from the counts in the control
-// block: B closes the director count (paccept, d) and advances the step, A
-// and F close the previous step's flip count (faccept).
-template <int PHASE>
-__device__ __forceinline__ void fused_control_update(Control* __restrict__ ctl, long long step) {
-  const float n3 = (float)ctl->nsites;
-  if (PHASE == kFusedB) {
-    const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
-    const float pa = (float)na / n3;  // chll_mod.f90:83
-    ctl->paccept = pa;
-    ctl->nacc_last = (long long)na;
-    ctl->nacc = 0;
-    if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
-    ctl->step = step + 1;
-  } else if (PHASE == kFusedA || PHASE == kFusedF) {
-    const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
-    ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
-    ctl->nflip_last = (long long)nf;
-    ctl->nflip = 0;
-  }
-}
-
 template <int PHASE>
 __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsigned int nacc,
                                                unsigned int nflip, long long step) {
@@ -176,20 +154,6 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
 // peer: the halo planes of neighbouring z-slabs that this slab's boundary
 // planes are written to (null pointers for a whole lattice).  The periodic
 // whole-lattice mode has no peers.
-// Programmatic dependent launch (sm_90+): the fused passes are launched so
-// that the next pass's grid may be scheduled while this one drains.  Each
-// pass first waits for the grids it depends on to complete and their memory
-// to be visible (griddepcontrol.wait, before any read of the lattice or the
-// control block), and lets its dependents launch once its own units are done
-// (griddepcontrol.launch_dependents, before the count epilogue).  Launches
-// without the attribute ignore both.
-__device__ __forceinline__ void wait_prerequisite_grids() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-__device__ __forceinline__ void allow_dependent_grids() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // FORM: 0 = grid-stride over units with padding checks, 1 = grid-stride, ni a
 // multiple of 4 (no padding), 2 = column walk (sweep_unit.cuh walk_task), ni a
 // multiple of 4.

@@ -12,6 +12,7 @@
 #pragma once
 #include "chll_common.cuh"
 #include "chll_physics.cuh"
+#include "sweep.cuh"
 
 namespace chll {
 
@@ -432,6 +433,42 @@ __host__ __device__ __forceinline__ double adapt_d(double d, float paccept) {
   if ((double)paccept < 0.4) return d * f;
   if ((double)paccept > 0.6) return d / f;
   return d;
+}
+
+// The control update after a fused pass (sweep.cuh FusedPhase), from the
+// counts in the control block: B closes the director count (paccept, d) and
+// advances the step, A and F close the previous step's flip count (faccept).
+template <int PHASE>
+__device__ __forceinline__ void fused_control_update(Control* __restrict__ ctl, long long step) {
+  const float n3 = (float)ctl->nsites;
+  if (PHASE == kFusedB) {
+    const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
+    const float pa = (float)na / n3;  // chll_mod.f90:83
+    ctl->paccept = pa;
+    ctl->nacc_last = (long long)na;
+    ctl->nacc = 0;
+    if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
+    ctl->step = step + 1;
+  } else if (PHASE == kFusedA || PHASE == kFusedF) {
+    const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
+    ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
+    ctl->nflip_last = (long long)nf;
+    ctl->nflip = 0;
+  }
+}
+
+// Programmatic dependent launch (sm_90+): pass kernels are launched so that
+// the next pass's grid may be scheduled while this one drains.  Each pass
+// first waits for the grids it depends on to complete and their memory to be
+// visible (griddepcontrol.wait, before any read of a lattice or a control
+// block), and lets its dependents launch once its own units are done
+// (griddepcontrol.launch_dependents, before the count epilogue).  Launches
+// without the attribute ignore both.
+__device__ __forceinline__ void wait_prerequisite_grids() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void allow_dependent_grids() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 }  // namespace chll

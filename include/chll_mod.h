@@ -250,6 +250,16 @@ int chll_batch_set_tuning(chll_batch* b, int threads, int ctas_per_sm);
  * (0, the default: all replicas in one wave), largest first; each wave gets
  * the whole co-resident grid, in the same launch. */
 int chll_batch_set_wave_bytes(chll_batch* b, int64_t wave_bytes);
+/* pooled = 1: chll_batch_run sweeps the replicas as pooled passes -- one
+ * launch per fused pass over all replicas' units, cut into equal blocks per
+ * CTA, the next pass launched as a programmatic dependent (CUDA graphs of
+ * measurement-interval chunks) -- instead of the persistent launch with
+ * software group barriers; 0 (the default unless chll_batch_autotune chose
+ * it): the persistent launch.  The chains are the same either way; the
+ * launch shape, waves and pairing apply to the persistent launch only.  No
+ * counterpart in the reference, which has no batched launch. */
+int chll_batch_set_pooled(chll_batch* b, int pooled);
+int chll_batch_get_pooled(chll_batch* b, int* pooled);
 /* pair = 1: the replicas of a wave are grouped two by two, by size, and each
  * group's CTAs alternate the two replicas' passes, so a wait at one
  * replica's group barrier overlaps the other replica's pass; 0 (the

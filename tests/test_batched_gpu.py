@@ -25,21 +25,22 @@ def _specs():
     ]
 
 
-@pytest.mark.parametrize("threads,wave_bytes,paired", [(128, 0, True), (128, 0, False),
-                                                       (256, 1, True), (512, 48 << 20, True),
-                                                       (128, 64 << 10, True),
-                                                       (256, 64 << 10, False)])
-def test_batch_replicas_equal_plain_runs(threads, wave_bytes, paired):
+@pytest.mark.parametrize("threads,wave_bytes,paired,pooled",
+                         [(128, 0, True, False), (128, 0, False, False), (256, 1, True, False),
+                          (512, 48 << 20, True, False), (128, 64 << 10, True, False),
+                          (256, 64 << 10, False, False), (256, 0, False, True)])
+def test_batch_replicas_equal_plain_runs(threads, wave_bytes, paired, pooled):
     """Any launch shape, wave split and grouping (two replicas alternating
-    their passes, or one) gives every replica its plain chain."""
+    their passes, or one) of the persistent launch, and the pooled passes,
+    give every replica its plain chain."""
     from chllmodel_b200.batched import Batch
     from chllmodel_b200.lattice import Lattice, coupling
 
     specs = _specs()
     nsw = 13
     with Batch(specs) as b:
-        b.set_tuning(threads, 0, wave_bytes, paired)
-        assert b.tuning()["paired"] == paired
+        b.set_tuning(threads, 0, wave_bytes, paired, pooled)
+        assert b.tuning()["paired"] == paired and b.tuning()["pooled"] == pooled
         if wave_bytes == 1:
             assert b.tuning()["waves"] == len(specs)  # every replica its own wave
         if wave_bytes == 64 << 10:
@@ -63,13 +64,15 @@ def test_batch_replicas_equal_plain_runs(threads, wave_bytes, paired):
         lat.close()
 
 
-def test_batch_measurements_equal_plain_observables():
+@pytest.mark.parametrize("pooled", [False, True])
+def test_batch_measurements_equal_plain_observables(pooled):
     from chllmodel_b200.batched import Batch
     from chllmodel_b200.lattice import Lattice, coupling
     from chllmodel_b200.observables import nematic_S
 
     specs = _specs()
     with Batch(specs) as b:
+        b.set_tuning(256, 0, pooled=pooled)
         b.init_random()
         b.run(10, measure_every=10)
         mom = b.moments()
