@@ -11,19 +11,24 @@
 // d, step, accept counters, barrier words and FP64 measurement accumulators.
 //
 // Schedule: the launch is sized to the co-resident CTA count (cooperative
-// launch), and every replica owns a contiguous group of CTAs proportional to
-// its number of sites (at least one).  A group walks its replica's units
-// grid-stride with the same sweep_unit() as the plain kernel, so a replica's
-// chain is bit-identical to the same replica run alone.  Between half-sweeps
-// the group meets at a software barrier in global memory (arrive counter +
-// generation word).  Every wait is bounded: on timeout the CTA sets the
-// replica's status word and returns, and so do the others at their next
-// barrier, so a fault ends the launch instead of hanging it.
+// launch), and every group of one replica (or, with pairing, two of
+// neighbouring sizes) owns a contiguous run of CTAs proportional to its
+// units (at least one).  A group walks its replica's units with the plain
+// kernels' code (the column walk or the grid-stride unit loop, as the cost
+// model picks for the group's thread count), so a replica's chain is
+// bit-identical to the same replica run alone.  Between passes the group
+// meets at a software barrier in global memory (arrive counter + generation
+// word), split into arrive and wait so that a paired group runs the other
+// replica's pass in between.  Every wait is bounded: on timeout the CTA sets
+// the replica's status word and returns, and so do the others at their next
+// barrier, so a fault ends the launch instead of hanging it.  The pooled
+// passes of pooled.cu are the alternative schedule (chll_batch_set_pooled).
 //
 // Measurements every `measure_every` sweeps (from sweep `measure_from`):
-// per-CTA FP64 moments (moments.cuh) -> partial slots -> the group's first
-// CTA sums them in a fixed order and accumulates e = E/N, eta = sum(s)/N and
-// the nematic order S = largest eigenvalue of Q = (3/2)<n n^T> - I/2.
+// per-CTA FP64 moments (moments.cuh) -> partial slots (two per CTA, one per
+// replica of its group) -> the group's first CTA sums them in a fixed order
+// and accumulates e = E/N, eta = sum(s)/N and the nematic order S = largest
+// eigenvalue of Q = (3/2)<n n^T> - I/2.
 #include <cuda_runtime.h>
 
 #include <algorithm>
