@@ -158,6 +158,10 @@ __device__ __forceinline__ void cta_sum3(unsigned int& a, unsigned int& b, unsig
   __syncthreads();
 }
 
+// The other colour is read through the coherent path (sweep_unit.cuh
+// ld_other): it was written by other CTAs of the group earlier in this launch.
+constexpr bool kCoherent = true;
+
 // One fused pass (sweep.cuh FusedPhase) of a replica by its CTA group: the
 // group's CTAs walk the replica's units grid-stride with the plain kernels'
 // unit_step, so the chain is the one the replica follows alone.
@@ -182,17 +186,16 @@ __device__ __noinline__ void group_loop(const ReplicaDesc& D, int rank, int nct,
   if (FULL && D.W.seg > 0) {
     const WalkGeom W = D.W;
     for (uint32_t t = (uint32_t)rank * THREADS + threadIdx.x; t < W.ntasks; t += stride)
-      walk_task<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, step, d, cp, key,
-                                                                     replica, nacc, nflip);
+      walk_task<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER, kCoherent>(
+          L, W, t, step, d, cp, key, replica, nacc, nflip);
     return;
   }
   const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
   const uint32_t per_colour = plane * (uint32_t)L.nk;
   for (uint32_t g = (uint32_t)rank * THREADS + threadIdx.x; g < G.units; g += stride) {
     if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-    unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER, FULL>(L, G, g, step, d, cp,
-                                                                         key, replica, nacc,
-                                                                         nflip);
+    unit_step<C, PERIODIC, PERIODIC, FLIP_BEFORE, DIR, FLIP_AFTER, FULL, kCoherent>(
+        L, G, g, step, d, cp, key, replica, nacc, nflip);
   }
 }
 

@@ -65,9 +65,8 @@ struct UnitSlots {
 };
 
 // Read-only path: the other colour's units, which no thread of the pass writes.
-// Not a compiler barrier: every pass is one kernel launch or one call of a
-// non-inlined group loop (batched.cu), so these loads cannot move into a
-// pass that writes what they read.
+// Not a compiler barrier: every pass that uses it is one kernel launch, so
+// these loads cannot move into a pass that writes what they read.
 __device__ __forceinline__ UnitSlots ld_unit_nc(const float4* p) {
   UnitSlots u;
   asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -88,6 +87,44 @@ __device__ __forceinline__ UnitSlots ld_unit(const float4* p) {
   return u;
 }
 
+// The other colour's reads come in two flavours, chosen by the template
+// argument COH of the unit code below.  COH = false: the read-only path
+// (ld.global.nc), valid where every pass is its own kernel launch (the
+// plain, slab and pooled passes: a launch boundary, or a programmatic
+// dependent's grid-dependency wait, orders one pass's stores before the next
+// pass's loads).  COH = true: weak ld.global, still cached in L1, for the
+// batched persistent launch, whose passes are separated by software barriers
+// inside one launch; there the release/acquire of the barrier orders the
+// stores of the pass before against these loads, which the memory model
+// guarantees for ld.global and not for the non-coherent path.  Not a
+// compiler barrier either: each batched pass is one call of a non-inlined
+// group loop, so the loads cannot move across the barrier between passes.
+__device__ __forceinline__ UnitSlots ld_unit_ca(const float4* p) {
+  UnitSlots u;
+  asm("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(u.a.x), "=f"(u.a.y), "=f"(u.a.z), "=f"(u.a.w), "=f"(u.b.x), "=f"(u.b.y),
+        "=f"(u.b.z), "=f"(u.b.w)
+      : "l"(p));
+  return u;
+}
+
+template <bool COH>
+__device__ __forceinline__ UnitSlots ld_other(const float4* p) {
+  return COH ? ld_unit_ca(p) : ld_unit_nc(p);
+}
+
+template <bool COH>
+__device__ __forceinline__ float4 ld4_other(const float4* p) {
+  if (COH) {
+    float4 v;
+    asm("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p));
+    return v;
+  }
+  return ld4(p);
+}
+
 __device__ __forceinline__ void st_unit(float4* p, const float4& a, const float4& b) {
   asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a.x), "f"(a.y),
                "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
@@ -95,9 +132,10 @@ __device__ __forceinline__ void st_unit(float4* p, const float4& a, const float4
 }
 
 // Neighbour unit pair, or zeros past an open boundary.
+template <bool COH = false>
 __device__ __forceinline__ void nbr_units(bool present, const float4* p, float4& s0, float4& s1) {
   if (present) {
-    const UnitSlots u = ld_unit_nc(p);
+    const UnitSlots u = ld_other<COH>(p);
     s0 = u.a;
     s1 = u.b;
   } else {
@@ -132,7 +170,7 @@ struct UnitNbhd {
 };
 
 // FULL: ni is a multiple of 4, so no unit holds a padding slot.
-template <int C, bool PXY, bool PZ, bool FULL = false>
+template <int C, bool PXY, bool PZ, bool FULL = false, bool COH = false>
 __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                             UnitNbhd& U) {
   const uint32_t hx = (uint32_t)L.hx;
@@ -180,18 +218,18 @@ __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeo
   U.fy = hjp;
   U.fz = hkp;
   const float4* orow = oth + rs;
-  const float4 fa = hxa ? ld4(orow + (xa >> 1)) : zero;
-  const float4 fb = hxb ? ld4(orow + (xb >> 1)) : zero;
-  const float4 fc = hxc ? ld4(orow + (xc >> 1)) : zero;
+  const float4 fa = hxa ? ld4_other<COH>(orow + (xa >> 1)) : zero;
+  const float4 fb = hxb ? ld4_other<COH>(orow + (xb >> 1)) : zero;
+  const float4 fc = hxc ? ld4_other<COH>(orow + (xc >> 1)) : zero;
   const uint32_t h0 = 2 * q;
   U.nb0.b[0] = fb;  // +x of i0
   U.nb0.b[1] = fa;  // -x of i0
   U.nb1.b[0] = fc;  // +x of i1
   U.nb1.b[1] = fb;  // -x of i1
-  nbr_units(hjp, oth + sjp + h0, U.nb0.b[2], U.nb1.b[2]);
-  nbr_units(hjm, oth + sjm + h0, U.nb0.b[3], U.nb1.b[3]);
-  nbr_units(hkp, oth + skp + h0, U.nb0.b[4], U.nb1.b[4]);
-  nbr_units(hkm, oth + skm + h0, U.nb0.b[5], U.nb1.b[5]);
+  nbr_units<COH>(hjp, oth + sjp + h0, U.nb0.b[2], U.nb1.b[2]);
+  nbr_units<COH>(hjm, oth + sjm + h0, U.nb0.b[3], U.nb1.b[3]);
+  nbr_units<COH>(hkp, oth + skp + h0, U.nb0.b[4], U.nb1.b[4]);
+  nbr_units<COH>(hkm, oth + skm + h0, U.nb0.b[5], U.nb1.b[5]);
 }
 
 // Where else an updated unit is written: nowhere (whole lattices), or, for a
@@ -219,14 +257,14 @@ struct PeerPlanes {
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.  A unit's slots are 2g (rows of hx = 2Q).
 template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
-          bool FULL = false, class KEY, class PEER = NoPeer>
+          bool FULL = false, bool COH = false, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica,
                                           unsigned int& nacc, unsigned int& nflip,
                                           const PEER& peer = PEER()) {
   UnitNbhd U;
-  gather_unit<C, PXY, PZ, FULL>(L, G, g, U);
+  gather_unit<C, PXY, PZ, FULL, COH>(L, G, g, U);
   unit_trials<C, FLIP_BEFORE, DIR, FLIP_AFTER>(U.n0, U.n1, U.nb0, U.nb1, U.v0, U.v1, g + G.goff,
                                                step, d, cp, key, replica, nacc, nflip);
   st_unit(U.cen, U.n0, U.n1);
@@ -318,8 +356,8 @@ __host__ inline double walk_pass_cost(uint32_t units, uint32_t ncols, uint32_t p
 
 // One task of the column walk: trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials on every unit of column t % ncols over its planes.
-template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER, class KEY,
-          class PEER = NoPeer>
+template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
+          bool COH = false, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& W, uint32_t t,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica, unsigned int& nacc,
@@ -355,7 +393,7 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
   // pair q of the x-row (j, k0)
   float4 xa, xb;
   {
-    const UnitSlots x = ld_unit_nc(oth + u);
+    const UnitSlots x = ld_other<COH>(oth + u);
     xa = x.a;
     xb = x.b;
   }
@@ -372,27 +410,27 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
     const UnitSlots ow = ld_unit(U.cen);
     U.n0 = ow.a;
     U.n1 = ow.b;
-    nbr_units(hyp, oth + (u + oyp), U.nb0.b[2], U.nb1.b[2]);
-    nbr_units(hym, oth + (u + oym), U.nb0.b[3], U.nb1.b[3]);
+    nbr_units<COH>(hyp, oth + (u + oyp), U.nb0.b[2], U.nb1.b[2]);
+    nbr_units<COH>(hym, oth + (u + oym), U.nb0.b[3], U.nb1.b[3]);
     float4 pa, pb;  // +z pair: the next step's x-row pair
-    nbr_units(hzp, oth + (u + ozp), pa, pb);
+    nbr_units<COH>(hzp, oth + (u + ozp), pa, pb);
     U.nb0.b[4] = pa;
     U.nb1.b[4] = pb;
     if (PZ || k > 0) {  // -z pair: this thread's x-row pair of the step before, from L1
-      const UnitSlots zr = ld_unit_nc(oth + (k > 0 ? u - plane : u + (nk - 1) * plane));
+      const UnitSlots zr = ld_other<COH>(oth + (k > 0 ? u - plane : u + (nk - 1) * plane));
       U.nb0.b[5] = zr.a;
       U.nb1.b[5] = zr.b;
     } else {
       U.nb0.b[5] = U.nb1.b[5] = zero;
     }
     if (o == 0) {
-      const float4 e = hx0 ? ld4(oth + (u + ox0)) : zero;
+      const float4 e = hx0 ? ld4_other<COH>(oth + (u + ox0)) : zero;
       U.nb0.b[0] = xa;  // +x of i0
       U.nb0.b[1] = e;   // -x of i0
       U.nb1.b[0] = xb;  // +x of i1
       U.nb1.b[1] = xa;  // -x of i1
     } else {
-      const float4 e = hx1 ? ld4(oth + (u + ox1)) : zero;
+      const float4 e = hx1 ? ld4_other<COH>(oth + (u + ox1)) : zero;
       U.nb0.b[0] = xb;  // +x of i0
       U.nb0.b[1] = xa;  // -x of i0
       U.nb1.b[0] = e;   // +x of i1

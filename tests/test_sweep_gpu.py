@@ -39,7 +39,10 @@ def lockstep(oracle, shape, periodic, kT, K, g, eps=1.0, sweeps=3, seed=5, d0=0.
     cp = coupling(kT, K, g, eps)
     ties = 0
     decided = 0
-    i, j, k = np.indices(shape)
+    ni, nj, nk = shape
+    parity = ((np.arange(ni, dtype=np.int32)[:, None, None] +
+               np.arange(nj, dtype=np.int32)[None, :, None] +
+               np.arange(nk, dtype=np.int32)[None, None, :]) & 1).astype(np.int8)
     for _ in range(sweeps):
         for p in range(4):
             ctl = lat.control()
@@ -51,7 +54,7 @@ def lockstep(oracle, shape, periodic, kT, K, g, eps=1.0, sweeps=3, seed=5, d0=0.
             d32 = float(np.float32(ctl["d"]))
             n, acc, de, u = oracle.run_pass(cfg, p, ctl["step"], d32, onx, ony, onz, os_,
                                             detail=True)
-            mine = ((i + j + k) & 1) == (p & 1)
+            mine = parity == (p & 1)
             # untouched colour
             for a, b in zip(after, before):
                 assert np.array_equal(a[~mine], b[~mine])
@@ -102,28 +105,75 @@ def test_lockstep_reference_size_run(oracle, periodic):
     as the reference's sweep and periodic, four sweeps in lockstep; then the
     library's fused sweep from the same start reaches the four half-sweeps'
     final GPU state and control block bit for bit."""
-    from chllmodel_b200.lattice import Lattice, coupling
-
     shape, nsw = (32, 32, 32), 4
     ties, decided = lockstep(oracle, shape, periodic, 0.5, 0.5, 0.0, sweeps=nsw, seed=1,
                              d0=0.1, init_seed=1)
     assert decided == 32 ** 3 * 2 * nsw
     assert ties <= max(2, decided // 2000)
+    assert _fused_equals_half_sweeps(oracle, shape, periodic, 0.5, 0.5, 0.0, nsw, 1)
+
+
+def _fused_equals_half_sweeps(oracle, shape, periodic, kT, K, g, nsw, seed, d0=0.1):
+    """From the oracle's initial state, the library's fused sweep (the column
+    walk where ni is a multiple of 4) and the four half-sweep kernels reach
+    the same state and control block bit for bit after nsw sweeps."""
+    from chllmodel_b200.lattice import Lattice, coupling
+
     bnd = "periodic" if periodic else "open"
-    nx, ny, nz, s = oracle.init_random(oracle.make_cfg(*shape, seed=1))
+    nx, ny, nz, s = oracle.init_random(oracle.make_cfg(*shape, seed=seed))
     four, fused = Lattice(*shape, boundary=bnd), Lattice(*shape, boundary=bnd)
-    cp = coupling(0.5, 0.5, 0.0)
+    cp = coupling(kT, K, g)
     for lat in (four, fused):
         lat.upload_f64(nx, ny, nz, s)
-        lat.set_control(0.1, step=1)
+        lat.set_control(d0, step=1)
     for _ in range(nsw):
         for p in range(4):
-            four.half_sweep(cp, p, seed=1)
-    fused.sweep(cp, nsw, seed=1)
-    assert np.array_equal(four.download_f4(), fused.download_f4())
-    assert four.control() == fused.control()
+            four.half_sweep(cp, p, seed=seed)
+    fused.sweep(cp, nsw, seed=seed)
+    same = np.array_equal(four.download_f4(), fused.download_f4())
+    ctl = four.control() == fused.control()
     four.close()
     fused.close()
+    return same and ctl
+
+
+# The other workloads' own lattices and couplings (periodic, eps = 1):
+# the 128^3 anneal (K = 1, h = 0.25, seed 7) at its first and last stage
+# temperatures, the 64^3 differentiation workload's equilibration (kT 0.3,
+# K = 1, h = 0.5, seed 3) and a 48^3 replica at two corners of the batched
+# phase grid (K = 1; kT 0.1, h 3.0 and kT 2.0, h 0.0).
+WORKLOAD_CASES = [
+    ((128, 128, 128), 1.5, 1.0, 0.25, 7, 2),
+    ((128, 128, 128), 0.1, 1.0, 0.25, 7, 2),
+    ((64, 64, 64), 0.3, 1.0, 0.5, 3, 3),
+    ((48, 48, 48), 0.1, 1.0, 3.0, 2, 3),
+    ((48, 48, 48), 2.0, 1.0, 0.0, 2, 3),
+]
+
+
+@pytest.mark.parametrize("shape,kT,K,g,seed,nsw", WORKLOAD_CASES)
+def test_lockstep_workload_lattices(oracle, shape, kT, K, g, seed, nsw):
+    """Lockstep against the oracle on the workloads' own lattice sizes and
+    couplings, then the fused sweep from the same start equal to the four
+    half-sweeps bit for bit."""
+    ties, decided = lockstep(oracle, shape, True, kT, K, g, sweeps=nsw, seed=seed, d0=0.1,
+                             init_seed=seed)
+    assert decided == int(np.prod(shape)) * 2 * nsw
+    assert ties <= max(2, decided // 2000)
+    assert _fused_equals_half_sweeps(oracle, shape, True, kT, K, g, nsw, seed)
+
+
+def test_lockstep_benchmark_lattice(oracle):
+    """The 480^3 benchmark lattice itself (periodic, K = 1, h = 0, kT = 0.3,
+    seed 11): one sweep in lockstep with the oracle (110.6 M sites), then one
+    fused sweep -- the benchmark's column-walk kernels -- equal to the four
+    half-sweep kernels bit for bit."""
+    shape = (480, 480, 480)
+    ties, decided = lockstep(oracle, shape, True, 0.3, 1.0, 0.0, sweeps=1, seed=11, d0=0.1,
+                             init_seed=11)
+    assert decided == 480 ** 3 * 2
+    assert ties <= max(2, decided // 2000)
+    assert _fused_equals_half_sweeps(oracle, shape, True, 0.3, 1.0, 0.0, 1, 11)
 
 
 def test_zero_temperature_rule(oracle):
