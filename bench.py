@@ -702,12 +702,17 @@ def batched_vs_plain(args, rank, torch):
     info_tune = b.tuning()
     b.close()
 
-    t_plain = float("nan")
-    for sp in ([] if args.no_plain_grid else specs):
-        if t_plain != t_plain:
-            t_plain = 0.0
+    # The same points one after another: the plain kernels launched pass by
+    # pass ("fused", the comparison the batched launch is measured against),
+    # and the library's default form per point ("auto": the resident cluster
+    # launch for the 32^3 points, the fused passes for the others).
+    t_seq = {"fused": float("nan"), "auto": float("nan")}
+    for kind, sp in [(k, sp) for k in t_seq for sp in ([] if args.no_plain_grid else specs)]:
+        if t_seq[kind] != t_seq[kind]:
+            t_seq[kind] = 0.0
         lat = Lattice(sp["ni"], sp["nj"], sp["nk"], boundary=sp["boundary"])
         lat.set_stream(stream.cuda_stream)
+        lat.set_kernel(kind)
         lat.init_random(sp["seed"], sp["replica"])
         lat.set_control(sp["d"], step=1)
         lat.reserve_rows(nsw // BATCH_NOUT + 1)
@@ -724,8 +729,9 @@ def batched_vs_plain(args, rank, torch):
             lat.measure(cp, c)
         a1.record(stream)
         a1.synchronize()
-        t_plain += a0.elapsed_time(a1) * 1e-3
+        t_seq[kind] += a0.elapsed_time(a1) * 1e-3
         lat.close()
+    t_plain = t_seq["fused"]
     # The same points as the reference's phase-diagram driver runs them: one
     # ChLLSim per point, run(nsweeps, BATCH_NOUT) through the C ABI with host
     # arrays (scripts/phase_diagram.py:25-31), wall time of each run summed.
@@ -747,6 +753,8 @@ def batched_vs_plain(args, rank, torch):
             "replicas": len(specs), "total_sites": total, "sweeps": nsw,
             "time_to_grid_s": t_batched, "sequential_plain_s": t_plain,
             "speedup_vs_sequential_plain": t_plain / t_batched,
+            "sequential_default_form_s": t_seq["auto"],
+            "speedup_vs_sequential_default_form": t_seq["auto"] / t_batched,
             "sequential_chllsim_s": t_sim,
             "speedup_vs_sequential_chllsim": t_sim / t_batched,
             "site_updates_per_s": total * nsw / t_batched,

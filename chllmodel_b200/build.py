@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchll_mod.so")
-SOURCES = ["sweep.cu", "batched.cu", "pooled.cu", "layout.cu", "observables.cu", "adjoint.cu",
-           "analysis.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["sweep.cu", "batched.cu", "pooled.cu", "resident.cu", "layout.cu", "observables.cu",
+           "adjoint.cu", "analysis.cu", "capi.cu", "noalloc.cu"]
 HEADERS = ["chll_common.cuh", "chll_physics.cuh", "sweep.cuh", "sweep_unit.cuh", "moments.cuh",
            "staged.cuh", "pooled.cuh"]
 

@@ -234,9 +234,25 @@ int get_graph(chll_lattice* L, const Coupling& cp, uint32_t k0, uint32_t k1, uin
     }
   }
   const LatticeView v = L->view();
+  // auto: the resident cluster launch where its threads hold at most one unit
+  // per pass (a pass is then mostly latency: 32^3 and below), else the fused
+  // passes (decided before the capture, which the cluster query must not meet)
+  const bool resident =
+      L->kernel == chll::kSweepResident ||
+      (L->kernel == chll::kSweepAuto && chll::resident_cluster() > 0 &&
+       chll::resident_units_per_thread(v) <= 1);
   cudaGraph_t graph = nullptr;
   CHLL_CUDA_TRY(cudaStreamBeginCapture(L->capture_stream, cudaStreamCaptureModeThreadLocal));
-  if (L->kernel == chll::kSweepAuto || L->kernel == chll::kSweepFused) {
+  if (resident) {
+    // the whole chunk in one cluster launch
+    if (chll::launch_resident_sweeps(v, cp, k0, k1, rep, L->ctl, nsweeps, L->capture_stream)) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(L->capture_stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return fail(CHLL_ECUDA, "resident sweep launch failed");
+    }
+  } else if (L->kernel == chll::kSweepAuto || L->kernel == chll::kSweepFused) {
     // A0 B (A B)... F: the fused two-pass sweep, flips completed at the end
     for (int s = 0; s < nsweeps; ++s) {
       chll::launch_fused_pass(v, cp, k0, k1, rep, L->ctl, s ? chll::kFusedA : chll::kFusedA0,
@@ -709,8 +725,12 @@ void chll_lattice_destroy(chll_lattice* L) {
 
 int chll_lattice_set_kernel(chll_lattice* L, int kernel) {
   if (!L) return fail(CHLL_EINVAL, "null lattice");
-  if (kernel < 0 || kernel > 3)
-    return fail(CHLL_EINVAL, "set_kernel: kernel must be 0, 1, 2 or 3");
+  if (kernel < 0 || kernel > 4)
+    return fail(CHLL_EINVAL, "set_kernel: kernel must be 0, 1, 2, 3 or 4");
+  if (kernel == chll::kSweepResident && L->slab)
+    return fail(CHLL_EINVAL, "set_kernel: a slab cannot run the resident form");
+  if (kernel == chll::kSweepResident && chll::resident_cluster() <= 0)
+    return fail(CHLL_ECUDA, "set_kernel: no thread-block cluster fits on this device");
   if (kernel == chll::kSweepStaged && !chll::staged_fits(L->view()))
     return fail(CHLL_EINVAL, "set_kernel: rows of %d sites are too long for the staged kernel",
                 L->ni);

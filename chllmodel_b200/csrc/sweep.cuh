@@ -9,11 +9,19 @@ namespace chll {
 // sweep.cu: per-device launch shapes (call once per device, outside any
 // stream capture) and one half-sweep (pass = kPassDir0..kPassSpin1).
 void sweep_prepare();
-// Sweep form: the two-pass fused sweep (auto), or the reference's four
+// Sweep form: the two-pass fused sweep, the fused passes of a chunk in one
+// cluster launch (resident.cu; auto picks it where each of its threads walks
+// at most one unit per pass, else the fused sweep), or the reference's four
 // half-sweeps with the direct kernel or the staged kernel (shared-memory
 // tiles by bulk copies).  All give the same chain.  Single half-sweeps
 // (chll_lattice_pass) use the direct kernel unless staged is chosen.
-enum SweepKernel : int { kSweepAuto = 0, kSweepDirect = 1, kSweepStaged = 2, kSweepFused = 3 };
+enum SweepKernel : int {
+  kSweepAuto = 0,
+  kSweepDirect = 1,
+  kSweepStaged = 2,
+  kSweepFused = 3,
+  kSweepResident = 4
+};
 void launch_sweep_pass(const LatticeView& L, const Coupling& cp, uint32_t key0, uint32_t key1,
                        uint32_t replica, Control* ctl, int pass, cudaStream_t stream,
                        int kernel = kSweepAuto);
@@ -36,6 +44,18 @@ void launch_fused_pass(const LatticeView& L, const SweepGeom& G, int bmode, cons
                        float4* peer_hi = nullptr);
 // The control update of a fused pass when the control block defers it.
 void launch_control_update(Control* ctl, int phase, cudaStream_t stream);
+
+// resident.cu: nsweeps fused sweeps of a whole lattice (A0 B (A B)... F, the
+// same chain and control block as the fused passes) in one launch of one
+// thread-block cluster whose CTAs meet at the cluster barrier between passes.
+// resident_cluster: CTAs of that cluster on this device (0: none fits);
+// resident_units_per_thread: units each of its threads walks per pass.
+// The launcher returns 0, or -1 if the launch failed.
+int resident_cluster();
+uint32_t resident_units_per_thread(const LatticeView& L);
+int launch_resident_sweeps(const LatticeView& L, const Coupling& cp, uint32_t key0,
+                           uint32_t key1, uint32_t replica, Control* ctl, int nsweeps,
+                           cudaStream_t stream);
 
 // layout.cu: natural-order (F-order, i fastest) <-> red/black float4.
 void launch_pack_f64(const LatticeView& L, const double* nx, const double* ny, const double* nz,

@@ -69,11 +69,14 @@ class Lattice:
         check(self._L.chll_lattice_set_stream(self._h, ct.c_void_p(stream_ptr or 0)))
 
     def set_kernel(self, kind: str) -> None:
-        """Sweep form: 'auto' (= 'fused'), 'fused' (two passes per sweep),
+        """Sweep form: 'auto' ('resident' up to about 32^3, else 'fused'),
+        'fused' (two passes per sweep),
         'direct' (the reference's four half-sweeps, neighbours from global
-        memory) or 'staged' (four half-sweeps from shared-memory row tiles).
-        All give the same chain bit for bit."""
-        code = {"auto": 0, "direct": 1, "staged": 2, "fused": 3}[kind]
+        memory), 'staged' (four half-sweeps from shared-memory row tiles) or
+        'resident' (the fused passes of a whole chunk in one thread-block
+        cluster launch, for small lattices).  All give the same chain bit for
+        bit."""
+        code = {"auto": 0, "direct": 1, "staged": 2, "fused": 3, "resident": 4}[kind]
         check(self._L.chll_lattice_set_kernel(self._h, code))
 
     def sync(self) -> None:

@@ -131,13 +131,19 @@ void chll_lattice_destroy(chll_lattice* lat);
  * the lattice's own stream; cudaStreamLegacy (0x1) selects the legacy default
  * stream). */
 int chll_lattice_set_stream(chll_lattice* lat, void* stream);
-/* Sweep form: 0 auto (= 3), 1 the reference's four half-sweeps per step with
+/* Sweep form: 0 auto (4 where each of its threads walks at most one unit per
+ * pass -- lattices up to about 32^3 -- else 3), 1 the reference's four
+ * half-sweeps per step with
  * neighbours read from global memory, 2 the four half-sweeps with row tiles
  * staged in shared memory by bulk copies, 3 the fused two-pass sweep (each
  * pass reads and writes every site once; the colour-0 flips of a step run at
- * the start of the next step's first pass, and after the last step).  All give
- * the same chain bit for bit.  chll_lattice_pass runs the staged kernel under
- * 2 and the direct kernel otherwise. */
+ * the start of the next step's first pass, and after the last step), 4 the
+ * fused passes of a whole chunk of steps in one launch of one thread-block
+ * cluster whose CTAs meet at the cluster barrier between passes (small
+ * lattices, where a pass is mostly launch and grid latency; refused for a slab
+ * and with CHLL_ECUDA where no cluster fits).  All give the same chain bit for
+ * bit.  chll_lattice_pass runs the staged kernel under 2 and the direct kernel
+ * otherwise. */
 int chll_lattice_set_kernel(chll_lattice* lat, int kernel);
 int chll_lattice_sync(chll_lattice* lat);
 /* Random initial state: directors uniform on the sphere, s = +-1 with p=1/2. */

@@ -122,6 +122,7 @@ def _fused_equals_half_sweeps(oracle, shape, periodic, kT, K, g, nsw, seed, d0=0
     bnd = "periodic" if periodic else "open"
     nx, ny, nz, s = oracle.init_random(oracle.make_cfg(*shape, seed=seed))
     four, fused = Lattice(*shape, boundary=bnd), Lattice(*shape, boundary=bnd)
+    fused.set_kernel("fused")
     cp = coupling(kT, K, g)
     for lat in (four, fused):
         lat.upload_f64(nx, ny, nz, s)
@@ -174,6 +175,34 @@ def test_lockstep_benchmark_lattice(oracle):
     assert decided == 480 ** 3 * 2
     assert ties <= max(2, decided // 2000)
     assert _fused_equals_half_sweeps(oracle, shape, True, 0.3, 1.0, 0.0, 1, 11)
+
+
+@pytest.mark.parametrize("shape,periodic", [((32, 32, 32), True), ((32, 32, 32), False),
+                                            ((48, 48, 48), True), ((30, 18, 10), False)])
+def test_resident_form_follows_the_chain(oracle, shape, periodic):
+    """The resident form (a chunk of sweeps in one cluster launch) on the
+    small workload sizes: the 32^3 configuration's couplings, chunks of 100
+    and 37 sweeps with a measurement row after each, equal to the fused
+    passes' state, control block and rows bit for bit."""
+    from chllmodel_b200.lattice import Lattice, coupling
+
+    nx, ny, nz, s = oracle.init_random(oracle.make_cfg(*shape, seed=1))
+    cp = coupling(0.5, 0.5, 0.0)
+    out = []
+    for kind in ("fused", "resident"):
+        lat = Lattice(*shape, boundary="periodic" if periodic else "open")
+        lat.set_kernel(kind)
+        lat.upload_f64(nx, ny, nz, s)
+        lat.set_control(0.1, step=1)
+        lat.reserve_rows(3)
+        for r, n in enumerate((100, 37, 100)):
+            lat.sweep(cp, n, seed=1)
+            lat.measure(cp, r)
+        out.append((lat.download_f4(), lat.control(), lat.read_rows(0, 3)))
+        lat.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
 
 
 def test_zero_temperature_rule(oracle):
@@ -292,15 +321,15 @@ def test_graph_replay_equals_single_passes(oracle):
                                             ((120, 6, 4), True), ((64, 64, 4), False)])
 def test_sweep_forms_follow_one_chain(shape, periodic):
     """The fused two-pass sweep, the four half-sweeps of the direct kernel,
-    the staged kernel, four single chll_lattice_pass calls per sweep and the
-    fused passes issued one by one all follow one chain bit for bit (same
-    units, counters and arithmetic), with the same control block (d, step,
-    paccept, faccept)."""
+    the staged kernel, the resident cluster launch, four single
+    chll_lattice_pass calls per sweep and the fused passes issued one by one
+    all follow one chain bit for bit (same units, counters and arithmetic),
+    with the same control block (d, step, paccept, faccept)."""
     from chllmodel_b200.lattice import FUSED_A, FUSED_A0, FUSED_B, FUSED_F, Lattice, coupling
 
     cp = coupling(0.6, 1.0, 0.2, 1.1)
     out = []
-    for kind in ("fused", "direct", "staged", "passes", "fused_passes"):
+    for kind in ("fused", "direct", "staged", "resident", "passes", "fused_passes"):
         lat = Lattice(*shape, boundary="periodic" if periodic else "open")
         if kind not in ("passes", "fused_passes"):
             lat.set_kernel(kind)
