@@ -160,7 +160,7 @@ __device__ __forceinline__ void cta_sum3(unsigned int& a, unsigned int& b, unsig
 
 // The other colour is read through the coherent path (sweep_unit.cuh
 // ld_other): it was written by other CTAs of the group earlier in this launch.
-constexpr bool kCoherent = true;
+constexpr int kCoherent = kLoadCoherent;
 
 // One fused pass (sweep.cuh FusedPhase) of a replica by its CTA group: the
 // group's CTAs walk the replica's units grid-stride with the plain kernels'

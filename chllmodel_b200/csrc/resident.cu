@@ -14,11 +14,11 @@
 // (fused_control_update), so the chain -- units, counters, arithmetic,
 // control block -- is the fused form's bit for bit.
 //
-// The other colour is read through the coherent path (sweep_unit.cuh COH =
-// true): it was written by other CTAs of the cluster earlier in the launch,
-// and the barrier's release/acquire orders those stores before the loads.
-// Each pass is one call of a non-inlined function, so no load can move
-// across the barrier between passes.
+// The other colour is read through the coherent path (sweep_unit.cuh
+// kLoadCoherentOrdered): it was written by other CTAs of the cluster earlier
+// in the launch, and the barrier's release/acquire orders those stores
+// before the loads; the loads carry a memory clobber, so the compiler cannot
+// move them across a barrier either.
 //
 // Launched without a programmatic-dependent attribute: a chunk is one launch.
 #include <cuda_runtime.h>
@@ -87,9 +87,10 @@ struct ResControl {
 };
 
 // One fused pass (sweep.cuh FusedPhase) over the lattice by the cluster's
-// threads: the plain kernels' column walk or unit loop, coherent loads.
+// threads: the plain kernels' column walk or unit loop, with coherent loads
+// that the compiler keeps between the barriers around the pass.
 template <int PHASE, int BMODE, int FORM>
-__device__ __noinline__ void resident_pass(const ResidentArgs& A, uint32_t rank, uint32_t step,
+__device__ __forceinline__ void resident_pass(const ResidentArgs& A, uint32_t rank, uint32_t step,
                                            float d, unsigned int& nacc, unsigned int& nflip) {
   constexpr int C = PHASE == kFusedB ? 1 : 0;
   constexpr bool FLIP_BEFORE = PHASE == kFusedA || PHASE == kFusedF;
@@ -106,16 +107,16 @@ __device__ __noinline__ void resident_pass(const ResidentArgs& A, uint32_t rank,
   if (FORM == 2) {
     const WalkGeom W = A.W;
     for (uint32_t t = rank * kResThreads + threadIdx.x; t < W.ntasks; t += stride)
-      walk_task<C, P, P, FLIP_BEFORE, DIR, FLIP_AFTER, true>(L, W, t, step, d, cp, key, replica,
-                                                             na, nf);
+      walk_task<C, P, P, FLIP_BEFORE, DIR, FLIP_AFTER, kLoadCoherentOrdered>(
+          L, W, t, step, d, cp, key, replica, na, nf);
   } else {
     const SweepGeom G = A.G;
     const uint32_t plane = (uint32_t)L.hx * (uint32_t)L.nj;
     const uint32_t per_colour = plane * (uint32_t)L.nk;
     for (uint32_t g = rank * kResThreads + threadIdx.x; g < G.units; g += stride) {
       if (g + stride < G.units) prefetch_unit<C>(L, g + stride, plane, per_colour);
-      unit_step<C, P, P, FLIP_BEFORE, DIR, FLIP_AFTER, FULL, true>(L, G, g, step, d, cp, key,
-                                                                   replica, na, nf);
+      unit_step<C, P, P, FLIP_BEFORE, DIR, FLIP_AFTER, FULL, kLoadCoherentOrdered>(
+          L, G, g, step, d, cp, key, replica, na, nf);
     }
   }
   nacc = na;

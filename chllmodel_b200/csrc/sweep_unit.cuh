@@ -87,18 +87,24 @@ __device__ __forceinline__ UnitSlots ld_unit(const float4* p) {
   return u;
 }
 
-// The other colour's reads come in two flavours, chosen by the template
-// argument COH of the unit code below.  COH = false: the read-only path
-// (ld.global.nc), valid where every pass is its own kernel launch (the
-// plain, slab and pooled passes: a launch boundary, or a programmatic
-// dependent's grid-dependency wait, orders one pass's stores before the next
-// pass's loads).  COH = true: weak ld.global, still cached in L1, for the
-// batched persistent launch, whose passes are separated by software barriers
-// inside one launch; there the release/acquire of the barrier orders the
-// stores of the pass before against these loads, which the memory model
-// guarantees for ld.global and not for the non-coherent path.  Not a
-// compiler barrier either: each batched pass is one call of a non-inlined
-// group loop, so the loads cannot move across the barrier between passes.
+// The other colour's reads come in three flavours, chosen by the template
+// argument COH of the unit code below.
+//   kLoadNc (0): the read-only path (ld.global.nc), valid where every pass is
+//     its own kernel launch (the plain, slab and pooled passes: a launch
+//     boundary, or a programmatic dependent's grid-dependency wait, orders
+//     one pass's stores before the next pass's loads).
+//   kLoadCoherent (1): weak ld.global, still cached in L1, for the batched
+//     persistent launch, whose passes are separated by software barriers
+//     inside one launch; there the release/acquire of the barrier orders the
+//     stores of the pass before against these loads, which the memory model
+//     guarantees for ld.global and not for the non-coherent path.  Not a
+//     compiler barrier: each batched pass is one call of a non-inlined group
+//     loop, so the loads cannot move across the barrier between passes.
+//   kLoadCoherentOrdered (2): the same loads with a memory clobber, for passes
+//     inlined between barriers (resident.cu): the compiler keeps them between
+//     the barriers around their pass.
+enum LoadMode : int { kLoadNc = 0, kLoadCoherent = 1, kLoadCoherentOrdered = 2 };
+
 __device__ __forceinline__ UnitSlots ld_unit_ca(const float4* p) {
   UnitSlots u;
   asm("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -108,15 +114,33 @@ __device__ __forceinline__ UnitSlots ld_unit_ca(const float4* p) {
   return u;
 }
 
-template <bool COH>
-__device__ __forceinline__ UnitSlots ld_other(const float4* p) {
-  return COH ? ld_unit_ca(p) : ld_unit_nc(p);
+__device__ __forceinline__ UnitSlots ld_unit_ca_ordered(const float4* p) {
+  UnitSlots u;
+  asm("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(u.a.x), "=f"(u.a.y), "=f"(u.a.z), "=f"(u.a.w), "=f"(u.b.x), "=f"(u.b.y),
+        "=f"(u.b.z), "=f"(u.b.w)
+      : "l"(p)
+      : "memory");
+  return u;
 }
 
-template <bool COH>
+template <int COH>
+__device__ __forceinline__ UnitSlots ld_other(const float4* p) {
+  if (COH == kLoadCoherentOrdered) return ld_unit_ca_ordered(p);
+  return COH == kLoadCoherent ? ld_unit_ca(p) : ld_unit_nc(p);
+}
+
+template <int COH>
 __device__ __forceinline__ float4 ld4_other(const float4* p) {
-  if (COH) {
-    float4 v;
+  float4 v;
+  if (COH == kLoadCoherentOrdered) {
+    asm("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p)
+        : "memory");
+    return v;
+  }
+  if (COH == kLoadCoherent) {
     asm("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];"
         : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
         : "l"(p));
@@ -132,7 +156,7 @@ __device__ __forceinline__ void st_unit(float4* p, const float4& a, const float4
 }
 
 // Neighbour unit pair, or zeros past an open boundary.
-template <bool COH = false>
+template <int COH = kLoadNc>
 __device__ __forceinline__ void nbr_units(bool present, const float4* p, float4& s0, float4& s1) {
   if (present) {
     const UnitSlots u = ld_other<COH>(p);
@@ -170,7 +194,7 @@ struct UnitNbhd {
 };
 
 // FULL: ni is a multiple of 4, so no unit holds a padding slot.
-template <int C, bool PXY, bool PZ, bool FULL = false, bool COH = false>
+template <int C, bool PXY, bool PZ, bool FULL = false, int COH = kLoadNc>
 __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                             UnitNbhd& U) {
   const uint32_t hx = (uint32_t)L.hx;
@@ -257,7 +281,7 @@ struct PeerPlanes {
 // unit_trials (chll_physics.cuh), adding accepted director trials to nacc
 // and accepted flips to nflip.  A unit's slots are 2g (rows of hx = 2Q).
 template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
-          bool FULL = false, bool COH = false, class KEY, class PEER = NoPeer>
+          bool FULL = false, int COH = kLoadNc, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void unit_step(const LatticeView& L, const SweepGeom& G, uint32_t g,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica,
@@ -357,7 +381,7 @@ __host__ inline double walk_pass_cost(uint32_t units, uint32_t ncols, uint32_t p
 // One task of the column walk: trials FLIP_BEFORE / DIR / FLIP_AFTER of
 // unit_trials on every unit of column t % ncols over its planes.
 template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
-          bool COH = false, class KEY, class PEER = NoPeer>
+          int COH = kLoadNc, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& W, uint32_t t,
                                           uint32_t step, float d, const Coupling& cp,
                                           const KEY& key, uint32_t replica, unsigned int& nacc,
