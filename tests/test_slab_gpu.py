@@ -76,6 +76,8 @@ def test_slab_rejects_whole_lattice_calls():
         sl.half_sweep(coupling(1.0, 1.0), 0)
     with pytest.raises(_lib.ChllError, match="slab"):
         sl.quench(coupling(1.0, 1.0), 0.1, 1)
+    with pytest.raises(_lib.ChllError, match="resident"):
+        sl.set_kernel("resident")
     sl.close()
 
 
