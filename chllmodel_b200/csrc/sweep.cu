@@ -167,6 +167,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   constexpr bool FLIP_AFTER = PHASE == kFusedB;
   constexpr bool PXY = BMODE != kBoundOpen;
   constexpr bool PZ = BMODE == kBoundPeriodic;
+  // the walk of a slab never leaves its storage in z (halo planes)
+  constexpr int WZ = BMODE == kBoundPeriodic ? kWalkZPeriodic
+                                             : (BMODE == kBoundSlabXY ? kWalkZHalo : kWalkZOpen);
   constexpr bool FULL = FORM != 0;
   wait_prerequisite_grids();
   const long long step = ctl->step;
@@ -178,11 +181,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (FORM == 2) {
     if (BMODE == kBoundPeriodic || (!peer.lo && !peer.hi)) {
       for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < W.ntasks; t += stride)
-        walk_task<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
+        walk_task<C, PXY, WZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
                                                             replica, nacc, nflip);
     } else {
       for (uint32_t t = blockIdx.x * kThreads + threadIdx.x; t < W.ntasks; t += stride)
-        walk_task<C, PXY, PZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
+        walk_task<C, PXY, WZ, FLIP_BEFORE, DIR, FLIP_AFTER>(L, W, t, (uint32_t)step, d, cp, keys,
                                                             replica, nacc, nflip, peer);
       // the halo stores reach the other GPU before this kernel counts as done
       __threadfence_system();

@@ -260,6 +260,7 @@ __device__ __forceinline__ void gather_unit(const LatticeView& L, const SweepGeo
 // z-slab, into the neighbouring slabs' halo planes.
 struct NoPeer {
   __device__ __forceinline__ void store(uint32_t, const float4&, const float4&) const {}
+  __device__ __forceinline__ void store_task_ends(const float4*, uint32_t, uint32_t) const {}
 };
 
 // A slab's first and last own planes of the pass's colour also go straight
@@ -274,6 +275,21 @@ struct PeerPlanes {
   __device__ __forceinline__ void store(uint32_t slot, const float4& n0, const float4& n1) const {
     if (lo && slot - lo_first < plane) st_unit(lo + (slot - lo_first), n0, n1);
     if (hi && slot - hi_first < plane) st_unit(hi + (slot - hi_first), n0, n1);
+  }
+  // After a column-walk task over planes: only its first unit can lie in the
+  // first own plane and only its last in the last own plane.  The units are
+  // read back (this thread wrote them) and stored to the halos, so that the
+  // walk's loop keeps no peer state in registers.
+  __device__ __forceinline__ void store_task_ends(const float4* own, uint32_t first_slot,
+                                                  uint32_t last_slot) const {
+    if (lo && first_slot - lo_first < plane) {
+      const UnitSlots v = ld_unit(own + first_slot);
+      st_unit(lo + (first_slot - lo_first), v.a, v.b);
+    }
+    if (hi && last_slot - hi_first < plane) {
+      const UnitSlots v = ld_unit(own + last_slot);
+      st_unit(hi + (last_slot - hi_first), v.a, v.b);
+    }
   }
 };
 
@@ -378,9 +394,15 @@ __host__ inline double walk_pass_cost(uint32_t units, uint32_t ncols, uint32_t p
   return best;
 }
 
+// z handling of the column walk: open (no neighbour past the first and last
+// plane), periodic (wrapped), or halo planes (a slab: the planes walked
+// always have both z neighbours in storage).
+enum WalkZ : int { kWalkZOpen = 0, kWalkZPeriodic = 1, kWalkZHalo = 2 };
+
 // One task of the column walk: trials FLIP_BEFORE / DIR / FLIP_AFTER of
-// unit_trials on every unit of column t % ncols over its planes.
-template <int C, bool PXY, bool PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
+// unit_trials on every unit of column t % ncols over its planes.  PZ is a
+// WalkZ (false / true for open / periodic).
+template <int C, bool PXY, int PZ, bool FLIP_BEFORE, bool DIR, bool FLIP_AFTER,
           int COH = kLoadNc, class KEY, class PEER = NoPeer>
 __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& W, uint32_t t,
                                           uint32_t step, float d, const Coupling& cp,
@@ -422,8 +444,10 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
     xb = x.b;
   }
   for (uint32_t k = k0; k < k1; ++k) {
-    const bool hzp = PZ || k + 1 < nk;
-    const uint32_t ozp = k + 1 < nk ? plane : (uint32_t)(-(int32_t)((nk - 1) * plane));
+    const bool hzp = PZ != kWalkZOpen || k + 1 < nk;
+    const uint32_t ozp = (PZ == kWalkZHalo || k + 1 < nk)
+                             ? plane
+                             : (uint32_t)(-(int32_t)((nk - 1) * plane));
     if (k + 1 < k1) {
       // the next step's own pair and +z pair, the lines no thread has read yet
       asm volatile("prefetch.global.L1 [%0];" ::"l"(own + (u + plane)));
@@ -440,8 +464,9 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
     nbr_units<COH>(hzp, oth + (u + ozp), pa, pb);
     U.nb0.b[4] = pa;
     U.nb1.b[4] = pb;
-    if (PZ || k > 0) {  // -z pair: this thread's x-row pair of the step before, from L1
-      const UnitSlots zr = ld_other<COH>(oth + (k > 0 ? u - plane : u + (nk - 1) * plane));
+    if (PZ != kWalkZOpen || k > 0) {  // -z pair: this thread's x-row pair of the step before
+      const UnitSlots zr = ld_other<COH>(
+          oth + ((PZ == kWalkZHalo || k > 0) ? u - plane : u + (nk - 1) * plane));
       U.nb0.b[5] = zr.a;
       U.nb1.b[5] = zr.b;
     } else {
@@ -464,13 +489,13 @@ __device__ __forceinline__ void walk_task(const LatticeView& L, const WalkGeom& 
                                                  g + W.goff, step, d, cp, key, replica, nacc,
                                                  nflip);
     st_unit(U.cen, U.n0, U.n1);
-    peer.store(u, U.n0, U.n1);
     xa = pa;
     xb = pb;
     u += plane;
     g += W.ncols;
     o ^= 1u;
   }
+  if (k1 > k0) peer.store_task_ends(own, u - (k1 - k0) * plane, u - plane);
 }
 
 // One of the reference's four half-sweeps on unit g; returns the number of

@@ -320,6 +320,12 @@ class TorchPeerHalo(TorchHalo):
     def sum_counts(self, index: int) -> None:
         self._all_reduce(self.counts[index:index + 1])
 
+    def exchange_and_sum(self, colour: int, index: int) -> None:
+        """After a pass that closes a count: the count's all-reduce is a
+        collective on the same stream after every rank's pass, so it orders
+        the passes (and the halo stores in them) as the token would."""
+        self.sum_counts(index)
+
     def close(self) -> None:
         """Unmaps the neighbours' allocations after the last pass; collective
         (every rank calls it before freeing its slab)."""
@@ -345,26 +351,36 @@ def sweep_slabs(slabs: list[SlabLattice], halo, cp, nsweeps: int, seed: int = 1,
     if nsweeps <= 0:
         return
     prime = getattr(halo, "prime", halo.exchange)  # the halos' first fill
+    # halo exchange plus the sum of the count the pass closed; a transport
+    # whose exchange is only an ordering collective does both in one
+    closing = getattr(halo, "exchange_and_sum", None)
+
+    def close(colour: int, index: int) -> None:
+        if closing is not None:
+            closing(colour, index)
+        else:
+            halo.exchange(colour)
+            halo.sum_counts(index)
+
     prime(0)
     prime(1)
     for s in range(nsweeps):
         for sl in slabs:
             sl.half_sweep(cp, FUSED_A if s else FUSED_A0, seed, replica)
-        halo.exchange(0)
         if s:  # pass A closed the previous step's flips
-            halo.sum_counts(1)
+            close(0, 1)
             for sl in slabs:
                 sl.control_update(FUSED_A)
+        else:
+            halo.exchange(0)
         for sl in slabs:
             sl.half_sweep(cp, FUSED_B, seed, replica)
-        halo.exchange(1)
-        halo.sum_counts(0)
+        close(1, 0)
         for sl in slabs:
             sl.control_update(FUSED_B)
     for sl in slabs:
         sl.half_sweep(cp, FUSED_F, seed, replica)
-    halo.exchange(0)
-    halo.sum_counts(1)
+    close(0, 1)
     for sl in slabs:
         sl.control_update(FUSED_F)
 
