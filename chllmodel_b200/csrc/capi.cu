@@ -234,14 +234,14 @@ int get_graph(chll_lattice* L, const Coupling& cp, uint32_t k0, uint32_t k1, uin
     }
   }
   const LatticeView v = L->view();
-  // auto: the resident cluster launch where its threads hold at most two
-  // units per pass (a pass is then mostly latency: up to about 40^3), else the
-  // fused passes (decided before the capture, which the cluster query must
-  // not meet)
+  // auto: the resident cluster launch where its threads hold at most one
+  // unit per pass (a pass is then mostly latency: up to 32^3), else the fused
+  // passes (decided before the capture, which the cluster query must not
+  // meet)
   const bool resident =
       L->kernel == chll::kSweepResident ||
       (L->kernel == chll::kSweepAuto && chll::resident_cluster() > 0 &&
-       chll::resident_units_per_thread(v) <= 2);
+       chll::resident_units_per_thread(v) <= 1);
   cudaGraph_t graph = nullptr;
   CHLL_CUDA_TRY(cudaStreamBeginCapture(L->capture_stream, cudaStreamCaptureModeThreadLocal));
   if (resident) {

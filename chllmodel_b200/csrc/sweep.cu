@@ -111,16 +111,27 @@ __global__ void __launch_bounds__(kThreads, 3)
 // state and draws the same counter.  Each site is read and written once per
 // pass, so a sweep moves half the bytes of the four-pass form.
 //
-// Control epilogue (last CTA): B closes the director count (paccept, d) and
-// advances the step; A and F close the previous sweep's flip count
-// (faccept), which B started with the colour-1 flips.
+// Control epilogue: B closes the director count (paccept, d) and advances the
+// step; A and F close the previous sweep's flip count (faccept), which B
+// started with the colour-1 flips.  Each CTA's thread 0 adds the CTA's
+// counts; the count the pass closes goes in together with one CTA ticket in
+// bits 40 and up of the same 64-bit word (counts stay below 2^40: at most
+// 2^32 sites), so the CTA that completes the grid's tickets has the pass total
+// in its own atomic's return value and runs the update at once: no fence, no
+// second read, no separate ticket word (the chain of fences and round trips
+// that cost ~2.7 us per pass at 32^3-96^3).  The other count is a plain add
+// for a later pass.  That CTA then clears the word -- or, on a slab whose
+// counts are summed over the slabs before the update (deferred), leaves the
+// bare total there.  A0 closes nothing and only adds.
+constexpr int kTicketShift = 40;
+constexpr unsigned long long kCountMask = (1ull << kTicketShift) - 1;
+
 template <int PHASE>
 __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsigned int nacc,
                                                unsigned int nflip, long long step) {
   constexpr bool DIR = PHASE != kFusedF;
   constexpr bool FLIPS = PHASE != kFusedA0;
   __shared__ unsigned int s_cnt[2];
-  __shared__ bool s_last;
   const int tid = threadIdx.x;
   if (tid < 2) s_cnt[tid] = 0;
   __syncthreads();
@@ -133,19 +144,31 @@ __device__ __forceinline__ void fused_epilogue(Control* __restrict__ ctl, unsign
     if ((tid & 31) == 0 && w) atomicAdd(&s_cnt[1], w);
   }
   __syncthreads();
-  if (tid == 0) {
-    if (DIR && s_cnt[0]) atomicAdd(&ctl->nacc, (unsigned long long)s_cnt[0]);
-    if (FLIPS && s_cnt[1]) atomicAdd(&ctl->nflip, (unsigned long long)s_cnt[1]);
-    __threadfence();
-    const unsigned int ticket = atomicAdd(&ctl->done, 1u);
-    s_last = (ticket == gridDim.x - 1);
+  if (tid != 0) return;
+  const unsigned long long na = s_cnt[0], nf = s_cnt[1];
+  if (PHASE == kFusedA0) {
+    if (na) atomicAdd(&ctl->nacc, na);
+    return;
   }
-  __syncthreads();
-  if (s_last && tid == 0) {
-    __threadfence();
-    ctl->done = 0;
-    if (!ctl->deferred) fused_control_update<PHASE>(ctl, step);
+  unsigned long long* closing = PHASE == kFusedB ? &ctl->nacc : &ctl->nflip;
+  const unsigned long long mine = PHASE == kFusedB ? na : nf;
+  if (PHASE == kFusedB) {
+    if (nf) atomicAdd(&ctl->nflip, nf);
+  } else if (DIR && na) {
+    atomicAdd(&ctl->nacc, na);
   }
+  // what the completing CTA needs, read before the ticket so that the loads
+  // overlap its round trip (no pass writes them)
+  const int deferred = ctl->deferred;
+  const long long nsites = ctl->nsites, adapt_until = ctl->adapt_until;
+  const double d = ctl->d;
+  const unsigned long long old = atomicAdd(closing, mine + (1ull << kTicketShift));
+  if ((old >> kTicketShift) != gridDim.x - 1) return;
+  const unsigned long long total = (old & kCountMask) + mine;
+  if (deferred)
+    *closing = total;
+  else
+    fused_close<PHASE>(ctl, total, step, nsites, adapt_until, d);
 }
 
 // Two CTAs per SM: the two sites' interleaved trials want up to 128

@@ -11,7 +11,7 @@ namespace chll {
 void sweep_prepare();
 // Sweep form: the two-pass fused sweep, the fused passes of a chunk in one
 // cluster launch (resident.cu; auto picks it where each of its threads walks
-// at most two units per pass, else the fused sweep), or the reference's four
+// at most one unit per pass, else the fused sweep), or the reference's four
 // half-sweeps with the direct kernel or the staged kernel (shared-memory
 // tiles by bulk copies).  All give the same chain.  Single half-sweeps
 // (chll_lattice_pass) use the direct kernel unless staged is chosen.

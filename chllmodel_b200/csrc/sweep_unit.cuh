@@ -525,23 +525,36 @@ __host__ __device__ __forceinline__ double adapt_d(double d, float paccept) {
 // The control update after a fused pass (sweep.cuh FusedPhase), from the
 // counts in the control block: B closes the director count (paccept, d) and
 // advances the step, A and F close the previous step's flip count (faccept).
+// The same update from a pass's closing total (B: director accepts of the
+// step, A and F: flips of the previous step) and the control block's fields
+// read beforehand (site count, adaptation limit, d).
 template <int PHASE>
-__device__ __forceinline__ void fused_control_update(Control* __restrict__ ctl, long long step) {
-  const float n3 = (float)ctl->nsites;
+__device__ __forceinline__ void fused_close(Control* __restrict__ ctl, unsigned long long total,
+                                            long long step, long long nsites,
+                                            long long adapt_until, double d) {
+  const float n3 = (float)nsites;
   if (PHASE == kFusedB) {
-    const unsigned long long na = atomicAdd(&ctl->nacc, 0ull);
-    const float pa = (float)na / n3;  // chll_mod.f90:83
+    const float pa = (float)total / n3;  // chll_mod.f90:83
     ctl->paccept = pa;
-    ctl->nacc_last = (long long)na;
+    ctl->nacc_last = (long long)total;
     ctl->nacc = 0;
-    if (step < ctl->adapt_until) ctl->d = adapt_d(ctl->d, pa);
+    if (step < adapt_until) ctl->d = adapt_d(d, pa);
     ctl->step = step + 1;
   } else if (PHASE == kFusedA || PHASE == kFusedF) {
-    const unsigned long long nf = atomicAdd(&ctl->nflip, 0ull);
-    ctl->faccept = (float)nf / n3;  // chll_mod.f90:93
-    ctl->nflip_last = (long long)nf;
+    ctl->faccept = (float)total / n3;  // chll_mod.f90:93
+    ctl->nflip_last = (long long)total;
     ctl->nflip = 0;
   }
+}
+
+template <int PHASE>
+__device__ __forceinline__ void fused_control_update(Control* __restrict__ ctl, long long step) {
+  if (PHASE == kFusedB)
+    fused_close<PHASE>(ctl, atomicAdd(&ctl->nacc, 0ull), step, ctl->nsites, ctl->adapt_until,
+                       ctl->d);
+  else if (PHASE == kFusedA || PHASE == kFusedF)
+    fused_close<PHASE>(ctl, atomicAdd(&ctl->nflip, 0ull), step, ctl->nsites, ctl->adapt_until,
+                       ctl->d);
 }
 
 // Programmatic dependent launch (sm_90+): pass kernels are launched so that

@@ -69,7 +69,7 @@ class Lattice:
         check(self._L.chll_lattice_set_stream(self._h, ct.c_void_p(stream_ptr or 0)))
 
     def set_kernel(self, kind: str) -> None:
-        """Sweep form: 'auto' ('resident' up to about 40^3, else 'fused'),
+        """Sweep form: 'auto' ('resident' up to about 32^3, else 'fused'),
         'fused' (two passes per sweep),
         'direct' (the reference's four half-sweeps, neighbours from global
         memory), 'staged' (four half-sweeps from shared-memory row tiles) or

@@ -131,8 +131,8 @@ void chll_lattice_destroy(chll_lattice* lat);
  * the lattice's own stream; cudaStreamLegacy (0x1) selects the legacy default
  * stream). */
 int chll_lattice_set_stream(chll_lattice* lat, void* stream);
-/* Sweep form: 0 auto (4 where each of its threads walks at most two units per
- * pass -- lattices up to about 40^3 -- else 3), 1 the reference's four
+/* Sweep form: 0 auto (4 where each of its threads walks at most one unit per
+ * pass -- lattices up to about 32^3 -- else 3), 1 the reference's four
  * half-sweeps per step with
  * neighbours read from global memory, 2 the four half-sweeps with row tiles
  * staged in shared memory by bulk copies, 3 the fused two-pass sweep (each
