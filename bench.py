@@ -226,9 +226,10 @@ def _oracle_lattice(edge, seed=SEED):
     return O, cfg, O.init_random(cfg)
 
 
-def cpu_sample(seconds: float, edge: int = L_EDGE):
+def cpu_sample(nsweeps: int, seconds: float, edge: int = L_EDGE):
     """Reference sweeps of the workload's edge^3 periodic lattice on the host
-    cores until `seconds` have elapsed (at least one sweep)."""
+    cores: `nsweeps` of them (10 at 480^3, about 15 s on 16 cores), stopping
+    early once `seconds` have elapsed (at least one sweep)."""
     O, cfg, (nx, ny, nz, s) = _oracle_lattice(edge)
     n = edge ** 3
     sweeps, t0, step = 0, time.perf_counter(), 1
@@ -238,7 +239,7 @@ def cpu_sample(seconds: float, edge: int = L_EDGE):
         step += 1
         sweeps += 1
         dt = time.perf_counter() - t0
-        if dt >= seconds:
+        if sweeps >= nsweeps or dt >= seconds:
             break
     return {"value": n * sweeps / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
             "sample": f"{sweeps} sweep(s) of the workload's {edge}^3 periodic lattice "
@@ -449,7 +450,7 @@ def gpu_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(args.cpu_seconds, edge)
+        cpu = cpu_sample(args.cpu_sweeps, args.cpu_seconds, edge)
 
     if dist is not None:
         dist.barrier()
@@ -573,7 +574,7 @@ def other_configs(args, torch):
     lat.close()
     cfg = O.make_cfg(e, e, e, periodic=True, kT=1.5, K=1.0, g=0.25, seed=7)
     ox, oy, oz, os_ = O.init_random(cfg)
-    ncpu = 60
+    ncpu = 100
     t0 = time.perf_counter()
     for st in range(1, ncpu + 1):
         for p in range(4):
@@ -883,7 +884,8 @@ def main():
                          "0 one replica per group (default: the library's)")
     ap.add_argument("--no-plain-grid", action="store_true",
                     help="skip the sequential plain-kernel grid (profiling runs)")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-sweeps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=30.0)
     ap.add_argument("--edge", type=int, default=L_EDGE,
                     help="lattice edge (480 is the benchmark; smaller edges for profiling)")
     args = ap.parse_args()
