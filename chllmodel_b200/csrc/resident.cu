@@ -2,8 +2,9 @@
 // launch of ONE thread-block cluster.
 //
 // A small lattice's fused pass is latency-bound: at 32^3 a pass holds 8,192
-// units, one per thread, and takes ~5 us from one launch to the next, most
-// of it the grid's start, drain and completion rather than its work.  Here
+// units, one per thread, and takes ~3.3 us from one launch to the next, most
+// of it the grid's start, drain, count epilogue and completion rather than
+// its work.  Here
 // the cluster's CTAs (up to 16, one per SM) stay resident for the whole
 // chunk and meet at the hardware cluster barrier between passes
 // (barrier.cluster.arrive.release / wait.acquire): no launch, no grid drain,
