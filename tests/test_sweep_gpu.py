@@ -138,30 +138,32 @@ def _fused_equals_half_sweeps(oracle, shape, periodic, kT, K, g, nsw, seed, d0=0
     return same and ctl
 
 
-# The other workloads' own lattices and couplings (periodic, eps = 1):
-# the 128^3 anneal (K = 1, h = 0.25, seed 7) at its first and last stage
-# temperatures, the 64^3 differentiation workload's equilibration (kT 0.3,
-# K = 1, h = 0.5, seed 3) and a 48^3 replica at two corners of the batched
-# phase grid (K = 1; kT 0.1, h 3.0 and kT 2.0, h 0.0).
+# The other workloads' own lattices and couplings (eps = 1): the 128^3
+# anneal (K = 1, h = 0.25, seed 7) at its first and last stage temperatures,
+# periodic, and its first stage with the reference's own open boundaries (the
+# default of ChLLSim); the 64^3 differentiation workload's equilibration
+# (kT 0.3, K = 1, h = 0.5, seed 3) and a 48^3 replica at two corners of the
+# batched phase grid (K = 1; kT 0.1, h 3.0 and kT 2.0, h 0.0), periodic.
 WORKLOAD_CASES = [
-    ((128, 128, 128), 1.5, 1.0, 0.25, 7, 2),
-    ((128, 128, 128), 0.1, 1.0, 0.25, 7, 2),
-    ((64, 64, 64), 0.3, 1.0, 0.5, 3, 3),
-    ((48, 48, 48), 0.1, 1.0, 3.0, 2, 3),
-    ((48, 48, 48), 2.0, 1.0, 0.0, 2, 3),
+    ((128, 128, 128), True, 1.5, 1.0, 0.25, 7, 2),
+    ((128, 128, 128), True, 0.1, 1.0, 0.25, 7, 2),
+    ((128, 128, 128), False, 1.5, 1.0, 0.25, 7, 2),
+    ((64, 64, 64), True, 0.3, 1.0, 0.5, 3, 3),
+    ((48, 48, 48), True, 0.1, 1.0, 3.0, 2, 3),
+    ((48, 48, 48), True, 2.0, 1.0, 0.0, 2, 3),
 ]
 
 
-@pytest.mark.parametrize("shape,kT,K,g,seed,nsw", WORKLOAD_CASES)
-def test_lockstep_workload_lattices(oracle, shape, kT, K, g, seed, nsw):
+@pytest.mark.parametrize("shape,periodic,kT,K,g,seed,nsw", WORKLOAD_CASES)
+def test_lockstep_workload_lattices(oracle, shape, periodic, kT, K, g, seed, nsw):
     """Lockstep against the oracle on the workloads' own lattice sizes and
     couplings, then the fused sweep from the same start equal to the four
     half-sweeps bit for bit."""
-    ties, decided = lockstep(oracle, shape, True, kT, K, g, sweeps=nsw, seed=seed, d0=0.1,
+    ties, decided = lockstep(oracle, shape, periodic, kT, K, g, sweeps=nsw, seed=seed, d0=0.1,
                              init_seed=seed)
     assert decided == int(np.prod(shape)) * 2 * nsw
     assert ties <= max(2, decided // 2000)
-    assert _fused_equals_half_sweeps(oracle, shape, True, kT, K, g, nsw, seed)
+    assert _fused_equals_half_sweeps(oracle, shape, periodic, kT, K, g, nsw, seed)
 
 
 def test_lockstep_benchmark_lattice(oracle):
