@@ -47,13 +47,27 @@ __global__ void __launch_bounds__(kObsThreads)
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  // The partials summed by the whole CTA: thread t takes blocks t, t + 256,
+  // ... (L2 reads, all in flight at once), then warp shuffles and the warps in
+  // order -- a fixed order for a given grid, so the result is reproducible.
+  double v[kObsMoments];
+#pragma unroll
+  for (int m = 0; m < kObsMoments; ++m) v[m] = 0.0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < kObsMoments; ++m) v[m] += __ldcg(&partials[(size_t)b * kObsMoments + m]);
+  }
+#pragma unroll
+  for (int m = 0; m < kObsMoments; ++m) {
+    const double w = warp_sum_d(v[m]);
+    if (lane == 0) s_part[warp][m] = w;
+  }
+  __syncthreads();
   __shared__ double s_tot[kObsMoments];
   if (threadIdx.x < kObsMoments) {
-    double v = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b) {
-      v += __ldcg(&partials[(size_t)b * kObsMoments + threadIdx.x]);  // L2, in block order
-    }
-    s_tot[threadIdx.x] = v;
+    double t = 0.0;
+    for (int w = 0; w < kObsThreads / 32; ++w) t += s_part[w][threadIdx.x];
+    s_tot[threadIdx.x] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
