@@ -119,7 +119,9 @@ __device__ __forceinline__ void site_sums(const float4& n, const float4& bx, con
 }
 
 // Block sums of the four FP64 accumulators into partials; the last block to
-// finish (ticket) adds the partials in block order into out4.
+// finish (ticket) adds the partials into out4 with all its threads (blocks
+// strided over the threads, then warp shuffles and the warps in order: a
+// fixed order for a given grid, so the sums are reproducible).
 __device__ __forceinline__ void finish_sums(const double acc[4], double* __restrict__ partials,
                                             unsigned int* __restrict__ ticket,
                                             double* __restrict__ out4) {
@@ -143,13 +145,22 @@ __device__ __forceinline__ void finish_sums(const double acc[4], double* __restr
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (threadIdx.x < 4) {
-    double v = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b)
-      v += __ldcg(&partials[(size_t)b * 4 + threadIdx.x]);  // L2, in block order
-    out4[threadIdx.x] = v;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) v[m] += __ldcg(&partials[(size_t)b * 4 + m]);  // L2
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const double w = warp_sum(v[m]);
+    if (lane == 0) s_part[warp][m] = w;
   }
   __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0.0;
+    for (int w = 0; w < kGradThreads / 32; ++w) t += s_part[w][threadIdx.x];
+    out4[threadIdx.x] = t;
+  }
   if (threadIdx.x == 0) *ticket = 0;
 }
 
